@@ -1,0 +1,373 @@
+#!/usr/bin/env python3
+"""Throughput of the negacyclic multiply c = a*b mod (X^N+1, q) at N=65536, W=1747 (L=55),
+bit-exact, on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--gemm tensor|plain]
+
+One step = one device-resident pass over a batch of BATCH multiplications whose operands
+are already in HBM (inputs 2 x BATCH x 14.4 MB > the 126 MB L2, so no flush is needed).
+Rank 0 prints one JSON line:
+  value       whole-job device-resident mults/s (tensor-core form unless --gemm plain),
+              CUDA events on the launching stream, max over ranks;
+  plain_value the same with the CUDA-core (plain int32) GEMM form, measured in the same run;
+  e2e         mults/s through the reference-facing call pm_run (fherma_run's C ABI) with
+              pageable host operands, host<->device copies inside the timed region, plus
+              p50/p99 latency of that call;
+  roofline    the dominant kernel's algorithmic bytes / its CUDA-event time vs measured HBM;
+  cpu_baseline the reference's own solve.cu (CPU-emulator build, oracle/_ref) on host cores.
+Multi-GPU: every rank multiplies its own batch (independent multiplications, no exchange):
+"scaling": "weak".
+--impl reference times the reference's CPU implementation alone (rank 0).
+"""
+import argparse
+import ctypes
+import datetime
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "polymult-challenge_b200")
+ORACLE = os.path.join(REPO, "oracle")
+sys.path.insert(0, PKG)
+
+N_RANK, W_RANK = 65536, 1747
+BATCH = 8
+METRIC = "mults/s at N=65536 W=1747 (bit-exact): tensor-core+batched vs plain; p99 ms"
+
+# algorithmic HBM bytes per launch of each kernel for ONE multiply (count=1):
+#   decomposition: N*L*4 in + K*N*4 out; column/row passes: K*N*4 in + out;
+#   fused row pass: 2*K*N*4 in + K*N*4 out; CRT: K*N*4 in + N*L*4 out
+def stage_bytes(stage, N, L, K):
+    rn, cw = K * N * 4, N * L * 4
+    return {"dec_a": cw + rn, "dec_b": cw + rn, "cols_a": 2 * rn, "cols_b": 2 * rn, "rows_a": 2 * rn,
+            "rows_fused": 3 * rn, "cols_inv": 2 * rn, "crt": rn + cw}[stage]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--gemm", default="tensor", choices=["tensor", "plain", "auto"])
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML (read-only) while running."""
+
+    def __init__(self, device_index):
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self._ok = True
+        except Exception:
+            pass
+
+    def _run(self):
+        nv = self.nv
+        names = {"hw_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwSlowdown", 0x8),
+                 "hw_thermal_slowdown": getattr(nv, "nvmlClocksThrottleReasonHwThermalSlowdown", 0x40),
+                 "sw_thermal_slowdown": getattr(nv, "nvmlClocksThrottleReasonSwThermalSlowdown", 0x20),
+                 "sw_power_cap": getattr(nv, "nvmlClocksThrottleReasonSwPowerCap", 0x4)}
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                for k, bit in names.items():
+                    if r & bit:
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self._ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._ok:
+            self.t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------------
+# CPU legs: the reference's own implementation (oracle/_ref), else the C restatement
+# ------------------------------------------------------------------------------------------
+def reference_cpu(N, W, q, a, b, calls, warm):
+    """Times fherma_run of the reference's solve.cu (CPU-emulator build). Returns dict."""
+    import numpy as np
+    L = (W + 31) // 32
+    qv = np.frombuffer(int(q).to_bytes(4 * L, "little"), dtype="<u4").copy()
+    so = os.path.join(ORACLE, "_ref", "libref_emu.so")
+    c = np.zeros((N, L), dtype=np.uint32)
+    if os.path.exists(so):
+        lib = ctypes.CDLL(so)
+        lib.ref_init.restype = ctypes.c_void_p
+        lib.ref_init.argtypes = [ctypes.c_uint32] * 3 + [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_run.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32] + [ctypes.c_void_p] * 3 + \
+            [ctypes.c_char_p, ctypes.c_int]
+        lib.ref_free.argtypes = [ctypes.c_void_p]
+        err = ctypes.create_string_buffer(256)
+        st = lib.ref_init(N, W, L, qv.ctypes.data, err, 256)
+        if not st:
+            raise RuntimeError("reference init failed: %s" % err.value)
+        times = []
+        for i in range(warm + calls):
+            t0 = time.perf_counter()
+            rc = lib.ref_run(st, N, L, a.ctypes.data, b.ctypes.data, c.ctypes.data, err, 256)
+            dt = time.perf_counter() - t0
+            if rc != 0:
+                raise RuntimeError("reference run failed: %s" % err.value)
+            if i >= warm:
+                times.append(dt)
+        lib.ref_free(st)
+        kind = "reference"
+        cores = 1
+        sample = ("%d fherma_run call(s) of the reference's solve.cu built against its CPU emulator pm_emu.h "
+                  "(kernels run on 1 thread; staging pool min(12, cpus-2) threads), N=%d W=%d" % (calls, N, W))
+    else:
+        lib = ctypes.CDLL(os.path.join(ORACLE, "_build", "librns_oracle.so"))
+        lib.orc_negacyclic_mul.argtypes = [ctypes.c_uint32] * 3 + [ctypes.c_void_p] * 4
+        times = []
+        for i in range(warm + calls):
+            t0 = time.perf_counter()
+            rc = lib.orc_negacyclic_mul(N, W, L, qv.ctypes.data, a.ctypes.data, b.ctypes.data, c.ctypes.data)
+            dt = time.perf_counter() - t0
+            if rc != 0:
+                raise RuntimeError("C oracle failed: %d" % rc)
+            if i >= warm:
+                times.append(dt)
+        kind = "port"
+        cores = os.cpu_count()
+        sample = "%d call(s) of the C restatement of the reference's RNS method (OpenMP), N=%d W=%d" % (calls, N, W)
+    return {"value": len(times) / sum(times), "unit": "mults/s", "cores": cores, "kind": kind, "sample": sample,
+            "host_cpus": os.cpu_count(), "seconds_per_call": statistics.median(times)}, c
+
+
+def run_reference(args):
+    world, rank, _ = dist_init()
+    if rank != 0:
+        return
+    import numpy as np
+    import workload
+    N, W = N_RANK, W_RANK
+    q = workload.spec_prime(N, W)
+    ops = workload.uniform_operands(N, W, q, 2, seed=7)
+    t0 = time.perf_counter()
+    cpu, _ = reference_cpu(N, W, q, np.ascontiguousarray(ops[0]), np.ascontiguousarray(ops[1]),
+                           calls=args.steps, warm=args.warmup)
+    total = time.perf_counter() - t0
+    line = {"metric": METRIC, "impl": "reference", "value": cpu["value"], "unit": "mults/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / cpu["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (uniform in [0,q), seeded)",
+            "config": {"workload": "negacyclic multiply N=65536 W=1747 L=55, one fherma_run per step",
+                       "N": N, "W": W, "L": 55},
+            "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "mults/s", "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0},
+            "wall_seconds": round(total, 1)}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+def time_device(torch, m, da, db, dc, batch, steps, warm):
+    stream = torch.cuda.current_stream()
+    for _ in range(warm):
+        m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), batch, stream.cuda_stream)
+    m.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), batch, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    m.sync()
+    return e0.elapsed_time(e1)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import polymult
+    import workload
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    N, W = N_RANK, W_RANK
+    L = (W + 31) // 32
+    q = workload.spec_prime(N, W)
+    qv = workload.limbs(q, L)
+    B = args.batch
+    host_a = workload.uniform_operands(N, W, q, B, seed=1000 + rank)
+    host_b = workload.uniform_operands(N, W, q, B, seed=2000 + rank)
+    da = torch.from_numpy(host_a.view(np.int32)).cuda()
+    db = torch.from_numpy(host_b.view(np.int32)).cuda()
+    dc = torch.zeros_like(da)
+
+    m = polymult.Multiplier(N, W, qv, gemm=args.gemm, device=local)
+    info = m.info()
+    # cross-check against the other form on one multiply before timing (outside the timed region)
+    other = "plain" if info["gemm"] == "tensor" else "tensor"
+    mp = polymult.Multiplier(N, W, qv, gemm=other, device=local)
+    dc2 = torch.zeros_like(dc)
+    stream = torch.cuda.current_stream().cuda_stream
+    m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), 1, stream)
+    mp.multiply_device(da.data_ptr(), db.data_ptr(), dc2.data_ptr(), 1, stream)
+    m.sync()
+    mp.sync()
+    forms_agree = bool(torch.equal(dc[0], dc2[0]))
+
+    barrier(world)
+    with ClockSampler(local) as clk:
+        ms = time_device(torch, m, da, db, dc, B, args.steps, args.warmup)
+    ms = max_over_ranks(ms, world)
+    value = world * args.steps * B / (ms / 1000.0)
+    groups_per_step = -(-B // max(1, info["group"]))
+    launches = args.steps * groups_per_step * info["launches_per_multiply"]
+
+    ms_plain = time_device(torch, mp, da, db, dc2, B, max(3, args.steps // 4), 2)
+    ms_plain = max_over_ranks(ms_plain, world)
+    plain_steps = max(3, args.steps // 4)
+    plain_value = world * plain_steps * B / (ms_plain / 1000.0)
+
+    # per-kernel times (count = 1 multiply) for the roofline
+    stages = m.time_stages(da.data_ptr(), db.data_ptr(), dc.data_ptr(), 1, 5, stream)
+    stages_plain = mp.time_stages(da.data_ptr(), db.data_ptr(), dc2.data_ptr(), 1, 3, stream)
+    dom = max(stages, key=stages.get)
+    K = info["K"]
+    alg = stage_bytes(dom, N, L, K)
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (stages[dom] / 1000.0) / 1e9
+    traffic = None
+    tfile = os.path.join(REPO, "profiles", "traffic_bytes.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(info["gemm"], {}).get(dom)
+        except Exception:
+            traffic = None
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes": alg, "kernel_ms": round(stages[dom], 4)}
+
+    # end to end through the reference-facing call (pageable host operands)
+    a0 = np.ascontiguousarray(host_a[0])
+    b0 = np.ascontiguousarray(host_b[0])
+    out = np.empty((N, L), dtype=np.uint32)
+    for _ in range(3):
+        m.multiply(a0, b0, out)
+    lat = []
+    barrier(world)
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        m.multiply(a0, b0, out)
+        lat.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(sum(lat), world)
+    e2e_ok = bool(np.array_equal(out, dc[0].cpu().numpy().view(np.uint32)))
+    lat_ms = sorted(x * 1000 for x in lat)
+    e2e = {"value": world * args.e2e_steps / e2e_s, "unit": "mults/s", "h2d_bytes_per_step": 2 * N * L * 4,
+           "d2h_bytes_per_step": N * L * 4, "p50_ms": round(lat_ms[len(lat_ms) // 2], 4),
+           "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 4),
+           "steps": args.e2e_steps, "matches_device_path": e2e_ok}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, cref = reference_cpu(N, W, q, a0, b0, calls=1, warm=0)
+        cpu["matches_gpu"] = bool(np.array_equal(cref, out))
+
+    m.close()
+    mp.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 2), "unit": "mults/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic (uniform in [0,q), seeded PCG64)",
+                "config": {"workload": "negacyclic multiply N=65536 W=1747 L=55 K=%d, device-resident batch of %d "
+                                       "per step" % (K, B), "N": N, "W": W, "L": L, "K": K, "batch_per_gpu": B,
+                           "gemm": info["gemm"], "parallelism": "replicas x%d" % world,
+                           "l2": "inputs larger than L2 (2 x %d x 14.4 MB), no flush" % B},
+                "plain_value": round(plain_value, 2), "tensor_over_plain": round(value / plain_value, 3),
+                "forms_agree": forms_agree,
+                "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+                "stages_ms_plain": {k: round(v, 4) for k, v in stages_plain.items()},
+                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,115 @@
+/*
+ * polymult_b200.h -- C ABI of the B200 negacyclic multiplier c = a*b mod (X^N + 1, q).
+ *
+ * Coefficients are W-bit integers in [0, q) stored as L = ceil(W/32) little-endian u32
+ * limbs; a polynomial is N x L words, row-major [N][L] (the reference's Tensor<u32> of
+ * shape {N, L}, fherma.h:31-40).  q must lie just below 2^W: delta = 2^W - q < 2^63 (the
+ * spec-derived prime: the largest prime below 2^W with q == 1 mod 2N).
+ *
+ * The reference binds three C++ symbols, fherma_init / fherma_run / fherma_free
+ * (fherma.h:45-48, fherma.toml:7-10).  This header is the plain-C boundary underneath
+ * them: pointers and sizes only, status codes instead of exceptions.  The C++ symbols
+ * themselves are declared in fherma_abi.h and implemented on top of these functions.
+ *
+ * Every call returns PM_OK (0) or a positive error code; pm_last_error() gives the
+ * message of the last failure on the calling thread.
+ */
+#ifndef POLYMULT_B200_H
+#define POLYMULT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pm_context pm_context;
+
+enum pm_status {
+    PM_OK = 0,
+    PM_ERR_INVALID = 1,     /* invalid point or argument (reference: runtime_error from precompute,
+                               solve.cu:873-913, or the size check of fherma_run, solve.cu:1482-1483) */
+    PM_ERR_CUDA = 2,        /* CUDA runtime failure (reference: check(), solve.cu:814-816) */
+    PM_ERR_DEVICE = 3,      /* a device-side check failed: CRT estimate bound, fold bound, wait timeout */
+    PM_ERR_UNSUPPORTED = 4, /* e.g. the tensor-core form requested for a point it does not cover */
+    PM_ERR_INTERNAL = 5
+};
+
+/* GEMM form of the RNS decomposition and the CRT. */
+enum pm_gemm_form {
+    PM_GEMM_AUTO = 0,   /* tensor cores where the point fits, else CUDA cores */
+    PM_GEMM_PLAIN = 1,  /* int32 CUDA-core kernels */
+    PM_GEMM_TENSOR = 2  /* tcgen05 kind::i8 byte-sliced GEMMs (error if the point does not fit) */
+};
+
+typedef struct pm_info {
+    uint32_t N, W, L;
+    int32_t K;             /* RNS primes */
+    int32_t logN, w1, w2;  /* 4-step split: nrows = 2^w1, ncols = 2^w2 */
+    int32_t gemm_form;     /* resolved form: PM_GEMM_PLAIN or PM_GEMM_TENSOR */
+    int32_t device;
+    uint64_t delta;        /* 2^W - q */
+    uint64_t table_bytes;  /* device memory of the per-point tables */
+    uint64_t scratch_bytes;/* device memory of the residue scratch */
+    int32_t launches_per_multiply; /* kernels launched per device-resident multiply group */
+    int32_t group;         /* multiplies per launch group of pm_run_device (scratch sized for it) */
+} pm_info;
+
+/* Replaces fherma_init (solve.cu:1392-1478): validates the point, builds every table,
+ * uploads them, allocates scratch and pinned staging, and runs one warm-up multiply. */
+int pm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_form, int device, pm_context** out);
+
+/* Replaces fherma_run (solve.cu:1480-1498): c = a*b for host operands through the chunked
+ * PCIe pipeline.  a, b, c: N*L words of host memory (pageable is fine).  Synchronous. */
+int pm_run(pm_context* ctx, const uint32_t* a, const uint32_t* b, uint32_t* c);
+
+/* No reference counterpart (the reference only takes host operands): c[i] = a[i]*b[i] for
+ * i < count, operands already in device memory as [count][N][L].  Asynchronous on
+ * `stream` (a cudaStream_t; NULL = legacy default stream); pm_sync() waits and reports
+ * device-side check failures. */
+int pm_run_device(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, uint32_t count,
+                  void* stream);
+
+/* Kernels of one device-resident multiply group, in launch order (pm_time_stages). */
+#define PM_STAGE_COUNT 8
+enum pm_stage {
+    PM_STAGE_DEC_A = 0,    /* RNS decomposition of a */
+    PM_STAGE_COLS_A = 1,   /* forward column pass of a */
+    PM_STAGE_ROWS_A = 2,   /* forward row pass of a */
+    PM_STAGE_DEC_B = 3,    /* RNS decomposition of b */
+    PM_STAGE_COLS_B = 4,   /* forward column pass of b */
+    PM_STAGE_FUSED = 5,    /* fused row pass: forward b, pointwise with a, inverse */
+    PM_STAGE_COLS_INV = 6, /* inverse column pass */
+    PM_STAGE_CRT = 7       /* CRT straight to mod q */
+};
+
+/* No reference counterpart (the reference's PM_PROFILE timer is host-side, solve.cu:1238-1242):
+ * runs `reps` device-resident multiply groups of `count` (<= pm_info.group) multiplies on
+ * `stream` and writes each kernel's mean duration in milliseconds, measured with CUDA events
+ * on that stream, to ms_out[PM_STAGE_COUNT].  Synchronous. */
+int pm_time_stages(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, uint32_t count,
+                   int reps, void* stream, float* ms_out);
+
+/* Waits for the context's device work and returns PM_ERR_DEVICE if a device-side check
+ * failed since the last call. */
+int pm_sync(pm_context* ctx);
+
+/* Replaces fherma_free (solve.cu:1530-1534). NULL is accepted. */
+void pm_free(pm_context* ctx);
+
+int pm_get_info(const pm_context* ctx, pm_info* out);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* pm_last_error(void);
+
+/* Host-only: builds the plan of a point without touching a GPU and runs its self-checks
+ * (primes, roots of unity, CRT reconstruction of random values through the tables).
+ * Fills *K_out with the prime count.  Usable on a machine without a GPU. */
+int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int32_t* K_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POLYMULT_B200_H */

@@ -1,0 +1,134 @@
+// pm_capi.cpp -- the extern "C" boundary (include/polymult_b200.h).  Exceptions never cross
+// it: each entry point maps them to a status code and keeps the message per thread.
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/polymult_b200.h"
+#include "pm_engine.h"
+
+struct pm_context {
+    pm::Engine* engine;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* what) {
+    g_last_error = what ? what : "";
+    return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return PM_OK;
+    } catch (const pm::InvalidPoint& e) {
+        return fail(PM_ERR_INVALID, e.what());
+    } catch (const pm::Unsupported& e) {
+        return fail(PM_ERR_UNSUPPORTED, e.what());
+    } catch (const pm::DeviceCheckError& e) {
+        return fail(PM_ERR_DEVICE, e.what());
+    } catch (const pm::CudaError& e) {
+        return fail(PM_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(PM_ERR_INTERNAL, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(PM_ERR_INTERNAL, e.what());
+    } catch (...) {
+        return fail(PM_ERR_INTERNAL, "unknown exception");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int pm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_form, int device, pm_context** out) {
+    if (!out) return fail(PM_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_TENSOR) return fail(PM_ERR_INVALID, "bad gemm_form");
+    return guarded([&] {
+        pm::Engine* e = new pm::Engine(N, W, L, q, gemm_form, device);
+        try {
+            // warm-up on zero operands: loads the module, touches every buffer
+            std::vector<uint32_t> zeros((size_t)N * L, 0), sink((size_t)N * L);
+            e->run_host(zeros.data(), zeros.data(), sink.data());
+        } catch (...) {
+            delete e;
+            throw;
+        }
+        *out = new pm_context{e};
+    });
+}
+
+int pm_run(pm_context* ctx, const uint32_t* a, const uint32_t* b, uint32_t* c) {
+    if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    if (!a || !b || !c) return fail(PM_ERR_INVALID, "null operand");
+    return guarded([&] { ctx->engine->run_host(a, b, c); });
+}
+
+int pm_run_device(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, uint32_t count,
+                  void* stream) {
+    if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    if (count && (!d_a || !d_b || !d_c)) return fail(PM_ERR_INVALID, "null operand");
+    return guarded([&] { ctx->engine->run_device(d_a, d_b, d_c, count, static_cast<cudaStream_t>(stream)); });
+}
+
+int pm_time_stages(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, uint32_t count,
+                   int reps, void* stream, float* ms_out) {
+    if (!ctx || !ctx->engine || !ms_out) return fail(PM_ERR_INVALID, "null argument");
+    if (!d_a || !d_b || !d_c) return fail(PM_ERR_INVALID, "null operand");
+    return guarded(
+        [&] { ctx->engine->time_stages(d_a, d_b, d_c, count, reps, static_cast<cudaStream_t>(stream), ms_out); });
+}
+
+int pm_sync(pm_context* ctx) {
+    if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    return guarded([&] { ctx->engine->throw_if_status(); });
+}
+
+void pm_free(pm_context* ctx) {
+    if (!ctx) return;
+    delete ctx->engine;
+    delete ctx;
+}
+
+int pm_get_info(const pm_context* ctx, pm_info* out) {
+    if (!ctx || !ctx->engine || !out) return fail(PM_ERR_INVALID, "null argument");
+    const pm::Engine& e = *ctx->engine;
+    const pm::Plan& P = e.plan();
+    std::memset(out, 0, sizeof *out);
+    out->N = P.N;
+    out->W = P.W;
+    out->L = P.L;
+    out->K = P.K;
+    out->logN = P.logN;
+    out->w1 = P.w1;
+    out->w2 = P.w2;
+    out->gemm_form = e.gemm_form();
+    out->device = e.device();
+    out->delta = P.delta;
+    out->table_bytes = e.table_bytes();
+    out->scratch_bytes = e.scratch_bytes();
+    out->launches_per_multiply = e.kernel_launches_per_group();
+    out->group = (int32_t)e.group();
+    return PM_OK;
+}
+
+const char* pm_last_error(void) { return g_last_error.c_str(); }
+
+int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int32_t* K_out) {
+    return guarded([&] {
+        pm::Plan P = pm::make_plan(N, W, L, q);
+        if (K_out) *K_out = P.K;
+        const std::string why = pm::check_plan(P);
+        if (!why.empty()) throw std::runtime_error("plan self-check failed: " + why);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// pm_device.cuh -- device-side parameters and modular arithmetic shared by every kernel.
+//
+// Residue arithmetic modulo p < 2^30 with R = 2^32:
+//   * Montgomery-Shoup product by a constant w held in Montgomery form (w R mod p) with its
+//     companion wc = w p^-1 mod 2^32: three integer multiplies, result in (0, 2p) for any
+//     32-bit multiplicand.  It replaces the reference's REDC-based mont_mul
+//     (solve.cu:123-130), which needs a 64-bit product and a wide add for every butterfly.
+//   * Harvey's lazy butterflies: forward values stay in [0, 4p), inverse values in [0, 2p),
+//     because 4p < 2^32.  The reference reduces to [0, p) after every butterfly
+//     (solve.cu:131-138, 230-241).
+#pragma once
+
+#include <cstdint>
+
+namespace pm {
+
+// Device status word bits (read back by the host after a run).
+enum : uint32_t {
+    DEV_ERR_CRT_BOUND = 1u,   // fp32 CRT estimate not within 1/4 of an integer (|x| < M/8 violated)
+    DEV_ERR_FOLD = 2u,        // delta-fold did not converge within its iteration bound
+    DEV_ERR_WAIT = 4u,        // an mbarrier wait hit its iteration limit
+};
+
+// Per-point device view of the plan.  POD, passed by value.
+struct DevPlan {
+    uint32_t N, nrows, ncols;
+    int logN, w1, w2;
+    int K, KP, L, W, HP;
+    uint64_t delta;
+    const uint32_t* p;        // [KP]
+    const uint32_t* pinv;     // [KP] p^-1 mod 2^32
+    const uint32_t* crt_c;    // [KP]
+    const uint32_t* crt_cc;   // [KP]
+    const float* rcp;         // [KP]
+    const uint32_t* tw;       // [K][N] Montgomery-form psi^bitrev(k)
+    const uint32_t* dec16;    // [2L][KP]
+    const uint16_t* qh16;     // [KP][HP]
+    const uint32_t* tneg;     // [K+1][L]
+    const uint32_t* q;        // [L]
+    const uint8_t* dec_b;     // tensor-core decomposition B operand (canonical image)
+    const uint8_t* crt_b;     // tensor-core CRT B operand (canonical image)
+    int dec_nrows, dec_kbytes;
+    int crt_nrows, crt_kbytes;
+    uint32_t* status;         // device status word
+};
+
+// A chunk of coefficient positions: all rows x `cw` columns starting at `col0`, stored
+// row-major as [row][column-in-chunk][limb].  With col0 = 0 and cw = ncols this is the
+// natural [N][L] layout.  Position pos maps to coefficient n = (pos / cw) * ncols + col0 + pos % cw.
+struct ChunkMap {
+    uint32_t col0, cw;
+    int lcw;  // log2(cw)
+};
+
+__device__ __forceinline__ uint32_t chunk_pos_to_n(const DevPlan& P, const ChunkMap& C, uint32_t pos) {
+    return ((pos >> C.lcw) << P.w2) + C.col0 + (pos & (C.cw - 1));
+}
+
+// x * w * 2^-32 mod p in (0, 2p); w < p in Montgomery form, wc = w * p^-1 mod 2^32.
+__device__ __forceinline__ uint32_t mul_ms(uint32_t x, uint32_t w, uint32_t wc, uint32_t p) {
+    const uint32_t m = x * wc;
+    return __umulhi(x, w) - __umulhi(m, p) + p;
+}
+
+// a * b * 2^-32 mod p in (0, 2p); requires a * b < p * 2^32.
+__device__ __forceinline__ uint32_t mont_mul(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
+    const uint32_t m = (a * b) * pinv;
+    return __umulhi(a, b) - __umulhi(m, p) + p;
+}
+
+// t * 2^-32 mod p in (0, 2p) for a 64-bit t < p * 2^32.
+__device__ __forceinline__ uint32_t redc64(uint64_t t, uint32_t p, uint32_t pinv) {
+    const uint32_t m = (uint32_t)t * pinv;
+    return (uint32_t)(t >> 32) - __umulhi(m, p) + p;
+}
+
+// [0, 2m) -> [0, m) (also [0, 4p) -> [0, 2p) with m = 2p): unsigned min of x and x - m.
+__device__ __forceinline__ uint32_t red_once(uint32_t x, uint32_t m) { return min(x, x - m); }
+
+struct Tw2 {
+    uint32_t w, wc;
+};
+
+__device__ __forceinline__ Tw2 make_tw(uint32_t w, uint32_t pinv) { return Tw2{w, w * pinv}; }
+
+// Cooley-Tukey (forward) Harvey butterfly: x, y in [0, 4p) -> x + wy, x - wy in [0, 4p).
+__device__ __forceinline__ void bfly_ct(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
+    const uint32_t p2 = 2 * p;
+    const uint32_t xr = red_once(x, p2);
+    const uint32_t t = mul_ms(y, w.w, w.wc, p);
+    x = xr + t;
+    y = xr - t + p2;
+}
+
+// Gentleman-Sande (inverse) butterfly with the mirrored twiddle: x, y in [0, 2p) ->
+// x + y, (y - x) w in [0, 2p).  (x - y) psi^-b = (y - x) psi^b' with b + b' = N.
+__device__ __forceinline__ void bfly_gs(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
+    const uint32_t p2 = 2 * p;
+    const uint32_t s = x + y;
+    const uint32_t d = y - x + p2;
+    x = red_once(s, p2);
+    y = mul_ms(d, w.w, w.wc, p);
+}
+
+__device__ __forceinline__ void flag_error(uint32_t* status, uint32_t bit) {
+    if (status) atomicOr(status, bit);
+}
+
+}  // namespace pm

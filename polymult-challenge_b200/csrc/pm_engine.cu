@@ -1,0 +1,563 @@
+// pm_engine.cu -- the multiply's runtime: device tables, scratch, launches, and the host
+// pipeline behind the reference-facing call.
+//
+// Device-resident multiply (run_device), per group of G multiplies sharing one launch each:
+//   decompose(a) -> column pass fwd(a) -> row pass fwd(a)
+//   decompose(b) -> column pass fwd(b) -> fused row pass (fwd b, * a, inv)
+//   column pass inv(b) -> CRT -> c
+// Host-operand multiply (run_host), the reference's chunked PCIe pipeline (solve.cu:1022-1243)
+// rebuilt around the same kernels: operands go in column chunks (the first NTT pass only
+// mixes coefficients within a column), each chunk gathered into pinned memory by the host
+// pool while the previous chunk's H2D copy, decomposition and column pass run; a's row pass
+// runs while b is still arriving; after b, the fused row pass; then per output column chunk
+// the inverse column pass, CRT and a D2H copy, each finished chunk scattered into the
+// caller's buffer while the next one is in flight.
+#include "pm_engine.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "pm_kernels.cuh"
+
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
+#include <sched.h>
+
+namespace pm {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------------------
+// host pool
+// ---------------------------------------------------------------------------------------
+HostPool::HostPool(int workers) {
+    for (int i = 0; i < workers; ++i) threads_.emplace_back([this] { loop(); });
+}
+
+HostPool::~HostPool() {
+    {
+        std::lock_guard<std::mutex> lk(m_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+}
+
+void HostPool::run(int n, const std::function<void(int)>& fn) {
+    if (n <= 0) return;
+    {
+        std::lock_guard<std::mutex> lk(m_);
+        fn_ = &fn;
+        n_ = n;
+        next_.store(0);
+        finished_ = 0;
+        ++gen_;
+    }
+    cv_.notify_all();
+    int done_here = 0;
+    for (int i = next_.fetch_add(1); i < n; i = next_.fetch_add(1)) {
+        fn(i);
+        ++done_here;
+    }
+    std::unique_lock<std::mutex> lk(m_);
+    finished_ += done_here;
+    done_cv_.wait(lk, [&] { return finished_ >= n_; });
+    fn_ = nullptr;
+}
+
+void HostPool::loop() {
+    uint64_t seen = 0;
+    for (;;) {
+        const std::function<void(int)>* fn;
+        int n;
+        {
+            std::unique_lock<std::mutex> lk(m_);
+            cv_.wait(lk, [&] { return stop_ || (gen_ != seen && fn_ != nullptr); });
+            if (stop_) return;
+            seen = gen_;
+            fn = fn_;
+            n = n_;
+        }
+        int done_here = 0;
+        for (int i = next_.fetch_add(1); i < n; i = next_.fetch_add(1)) {
+            (*fn)(i);
+            ++done_here;
+        }
+        std::lock_guard<std::mutex> lk(m_);
+        finished_ += done_here;
+        if (finished_ >= n_) done_cv_.notify_all();
+    }
+}
+
+namespace {
+
+int usable_cpus() {
+    cpu_set_t set;
+    if (sched_getaffinity(0, sizeof(set), &set) == 0) return CPU_COUNT(&set);
+    return (int)std::max(1u, std::thread::hardware_concurrency());
+}
+
+// pageable <-> pinned copy with non-temporal stores where aligned (the destination is not
+// read back by this thread, so skipping its read-for-ownership saves host bandwidth)
+void stream_copy(void* dst, const void* src, size_t bytes) {
+#if defined(__x86_64__)
+    if (((uintptr_t)dst & 15) == 0 && (bytes & 15) == 0) {
+        __m128i* d = static_cast<__m128i*>(dst);
+        const __m128i* s = static_cast<const __m128i*>(src);
+        const size_t n = bytes / 16;
+        for (size_t i = 0; i < n; ++i) _mm_stream_si128(d + i, _mm_loadu_si128(s + i));
+        _mm_sfence();
+        return;
+    }
+#endif
+    std::memcpy(dst, src, bytes);
+}
+
+// `n` column chunks covering [0, ncols): power-of-two widths, narrow ones at the ends named
+// by `head` / `tail` (fractions 1/d of ncols) so that the pipeline fills and drains sooner.
+std::vector<Chunk> make_chunks(uint32_t ncols, std::initializer_list<uint32_t> head, uint32_t body,
+                               std::initializer_list<uint32_t> tail) {
+    std::vector<uint32_t> w, t;
+    uint32_t rem = ncols;
+    for (uint32_t d : head) {
+        const uint32_t x = std::min(rem, std::max(1u, ncols / d));
+        if (x && rem > x) {
+            w.push_back(x);
+            rem -= x;
+        }
+    }
+    uint32_t tsum = 0;
+    for (uint32_t d : tail) {
+        const uint32_t x = std::max(1u, ncols / d);
+        if (tsum + x < rem) {
+            t.push_back(x);
+            tsum += x;
+        }
+    }
+    const uint32_t bw = std::max(1u, ncols / body);
+    while (rem > tsum) {
+        uint32_t x = std::min(bw, rem - tsum);
+        // keep widths powers of two (chunk_pos_to_n divides by cw with a shift)
+        while (x & (x - 1)) x &= x - 1;
+        w.push_back(x);
+        rem -= x;
+    }
+    w.insert(w.end(), t.begin(), t.end());
+    std::vector<Chunk> out;
+    uint32_t col = 0;
+    for (uint32_t x : w) {
+        out.push_back({col, x});
+        col += x;
+    }
+    return out;
+}
+
+int ilog2(uint32_t x) {
+    int l = 0;
+    while ((1u << l) < x) ++l;
+    return l;
+}
+
+template <class T>
+T* dev_alloc(std::vector<void*>& keep, size_t count, size_t* total) {
+    T* d = nullptr;
+    cuda_check(cudaMalloc(&d, std::max<size_t>(1, count) * sizeof(T)), "cudaMalloc");
+    keep.push_back(d);
+    if (total) *total += count * sizeof(T);
+    return d;
+}
+
+template <class T>
+T* dev_upload(std::vector<void*>& keep, const std::vector<T>& v, size_t* total) {
+    T* d = dev_alloc<T>(keep, v.size(), total);
+    if (!v.empty()) cuda_check(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    return d;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// construction
+// ---------------------------------------------------------------------------------------
+Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_request, int device)
+    : plan_(make_plan(N, W, L, q)), device_(device) {
+    int ndev = 0;
+    cuda_check(cudaGetDeviceCount(&ndev), "no CUDA device");
+    if (device < 0 || device >= ndev) throw CudaError("device index out of range");
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    cuda_check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major != 10) throw Unsupported("this library is built for sm_100a (B200); device is sm_" +
+                                            std::to_string(prop.major * 10 + prop.minor));
+    num_sms_ = prop.multiProcessorCount;
+    smem_optin_ = prop.sharedMemPerBlockOptin;
+    try {
+        upload_tables();
+        setup_launch_shapes();
+        const bool tc_fits = rns_tc_smem(dp_) <= smem_optin_ && crt_tc_smem(dp_) <= smem_optin_ &&
+                             dp_.dec_nrows <= 512 && dp_.crt_nrows <= 512;
+        if (gemm_request == GEMM_TENSOR && !tc_fits)
+            throw Unsupported("tensor-core GEMM form does not cover this point (shared memory / TMEM)");
+        form_ = (gemm_request == GEMM_PLAIN || !tc_fits) ? GEMM_PLAIN : GEMM_TENSOR;
+        if (form_ == GEMM_TENSOR) {
+            smem_dec_ = rns_tc_smem(dp_);
+            smem_crt_ = crt_tc_smem(dp_);
+        }
+        // one multiply's worth of residues per group at the ranked size; more for small N
+        const size_t per_mult = (size_t)plan_.K * plan_.N;
+        group_cap_ = (uint32_t)std::max<size_t>(1, std::min<size_t>(256, (8u << 20) / std::max<size_t>(1, per_mult)));
+        ensure_scratch(1);
+        setup_host_pipeline();
+    } catch (...) {
+        for (void* d : dev_allocs_) cudaFree(d);
+        dev_allocs_.clear();
+        throw;
+    }
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    cudaDeviceSynchronize();
+    pool_.reset();
+    for (auto e : ev_in_) cudaEventDestroy(e);
+    for (auto e : ev_done_in_) cudaEventDestroy(e);
+    for (auto e : ev_crt_) cudaEventDestroy(e);
+    for (auto e : ev_out_) cudaEventDestroy(e);
+    if (ev_row_a_) cudaEventDestroy(ev_row_a_);
+    if (ev_fused_) cudaEventDestroy(ev_fused_);
+    for (auto s : s_comp_)
+        if (s) cudaStreamDestroy(s);
+    if (s_h2d_) cudaStreamDestroy(s_h2d_);
+    if (s_d2h_) cudaStreamDestroy(s_d2h_);
+    for (void* d : dev_allocs_) cudaFree(d);
+    if (d_ra_) cudaFree(d_ra_);
+    if (d_rb_) cudaFree(d_rb_);
+    for (auto h : h_in_)
+        if (h) cudaFreeHost(h);
+    if (h_out_) cudaFreeHost(h_out_);
+}
+
+void Engine::upload_tables() {
+    const Plan& P = plan_;
+    DevPlan& d = dp_;
+    d.N = P.N;
+    d.nrows = P.nrows;
+    d.ncols = P.ncols;
+    d.logN = P.logN;
+    d.w1 = P.w1;
+    d.w2 = P.w2;
+    d.K = P.K;
+    d.KP = P.KP;
+    d.L = (int)P.L;
+    d.W = (int)P.W;
+    d.HP = P.HP;
+    d.delta = P.delta;
+    size_t* tb = &table_bytes_;
+    d.p = dev_upload(dev_allocs_, P.p, tb);
+    d.pinv = dev_upload(dev_allocs_, P.pinv, tb);
+    d.crt_c = dev_upload(dev_allocs_, P.crt_c, tb);
+    d.crt_cc = dev_upload(dev_allocs_, P.crt_cc, tb);
+    d.rcp = dev_upload(dev_allocs_, P.rcp, tb);
+    d.tw = dev_upload(dev_allocs_, P.tw, tb);
+    d.dec16 = dev_upload(dev_allocs_, P.dec16, tb);
+    d.qh16 = dev_upload(dev_allocs_, P.qh16, tb);
+    d.tneg = dev_upload(dev_allocs_, P.tneg, tb);
+    d.q = dev_upload(dev_allocs_, P.q, tb);
+    d.dec_b = dev_upload(dev_allocs_, P.dec_b, tb);
+    d.crt_b = dev_upload(dev_allocs_, P.crt_b, tb);
+    d.dec_nrows = P.dec_gemm.n_rows;
+    d.dec_kbytes = P.dec_gemm.k_bytes;
+    d.crt_nrows = P.crt_gemm.n_rows;
+    d.crt_kbytes = P.crt_gemm.k_bytes;
+    uint32_t* st = dev_alloc<uint32_t>(dev_allocs_, 1, nullptr);
+    cuda_check(cudaMemset(st, 0, 4), "memset status");
+    d.status = st;
+}
+
+void Engine::setup_launch_shapes() {
+    rpb_ = (int)std::min<uint32_t>(plan_.nrows, std::max<uint32_t>(1, 1024 / plan_.ncols));
+    smem_cols_ = ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(32, plan_.ncols)));
+    smem_rows_fwd_ = ntt_rows_smem(dp_, rpb_, false);
+    smem_rows_fused_ = ntt_rows_smem(dp_, rpb_, true);
+    if (smem_cols_ > smem_optin_ || smem_rows_fused_ > smem_optin_) throw Unsupported("NTT tile exceeds shared memory");
+    dec_tab_smem_ = rns_plain_smem(dp_, true) <= 100 * 1024;
+    smem_dec_ = rns_plain_smem(dp_, dec_tab_smem_);
+    smem_crt_ = crt_plain_smem(dp_);
+    if (smem_dec_ > smem_optin_ || smem_crt_ > smem_optin_) throw Unsupported("plain GEMM tile exceeds shared memory");
+    // Every kernel may use up to the device's opt-in maximum: contexts for different points
+    // share these kernels, so a per-point limit set by one context could fail another's launch.
+    const int mx = (int)smem_optin_;
+    cuda_check(cudaFuncSetAttribute(k_ntt_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_ntt_cols<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_ntt_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_ntt_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_rns_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_crt_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_rns_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_crt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+}
+
+void Engine::ensure_scratch(uint32_t group) {
+    if (group <= group_) return;
+    if (d_ra_) cudaFree(d_ra_);
+    if (d_rb_) cudaFree(d_rb_);
+    d_ra_ = d_rb_ = nullptr;
+    const size_t words = (size_t)group * plan_.K * plan_.N;
+    cuda_check(cudaMalloc(&d_ra_, words * 4), "cudaMalloc residues");
+    cuda_check(cudaMalloc(&d_rb_, words * 4), "cudaMalloc residues");
+    scratch_words_ = 2 * words;
+    group_ = group;
+}
+
+void Engine::setup_host_pipeline() {
+    const uint32_t nc = plan_.ncols;
+    cin_ = make_chunks(nc, {32, 32, 16}, 8, {});
+    cout_ = make_chunks(nc, {64, 64, 32}, 16, {32, 64, 64});
+    const size_t bytes = plan_.coeff_words() * 4;
+    for (int i = 0; i < 2; ++i) {
+        d_in_[i] = dev_alloc<uint32_t>(dev_allocs_, plan_.coeff_words(), nullptr);
+        cuda_check(cudaHostAlloc(&h_in_[i], bytes, cudaHostAllocDefault), "cudaHostAlloc");
+    }
+    d_out_ = dev_alloc<uint32_t>(dev_allocs_, plan_.coeff_words(), nullptr);
+    cuda_check(cudaHostAlloc(&h_out_, bytes, cudaHostAllocDefault), "cudaHostAlloc");
+    for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
+    cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
+    auto mk = [](std::vector<cudaEvent_t>& v, size_t n) {
+        v.resize(n);
+        for (auto& e : v) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    };
+    mk(ev_in_, 2 * cin_.size());
+    mk(ev_done_in_, 2 * cin_.size());
+    mk(ev_crt_, cout_.size());
+    mk(ev_out_, cout_.size());
+    cuda_check(cudaEventCreateWithFlags(&ev_row_a_, cudaEventDisableTiming), "event");
+    cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
+    pool_.reset(new HostPool(std::max(0, std::min(12, usable_cpus() - 2))));
+}
+
+int Engine::kernel_launches_per_group() const { return plan_.w1 > 0 ? 8 : 6; }
+
+ChunkMap Engine::chunk_map(Chunk ch) const {
+    ChunkMap m;
+    m.col0 = ch.col0;
+    m.cw = ch.cw;
+    m.lcw = ilog2(ch.cw);
+    return m;
+}
+
+// ---------------------------------------------------------------------------------------
+// launches
+// ---------------------------------------------------------------------------------------
+void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s) const {
+    const uint32_t npos = plan_.nrows * ch.cw;
+    if (form_ == GEMM_TENSOR) {
+        const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
+        const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
+        k_rns_tc<<<grid, 128, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, nb, R);
+    } else {
+        dim3 grid((npos + DEC_TM - 1) / DEC_TM, 1, nb);
+        k_rns_plain<<<grid, 256, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, R, dec_tab_smem_ ? 1 : 0);
+    }
+}
+
+void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s) const {
+    if (plan_.w1 == 0) return;
+    const int ltc = ilog2(std::min<uint32_t>(32, ch.cw));
+    dim3 grid(ch.cw >> ltc, plan_.K, nb);
+    const size_t smem = ntt_cols_smem(dp_, ltc);
+    if (inv) k_ntt_cols<true><<<grid, 256, smem, s>>>(dp_, R, ch.col0, ltc);
+    else k_ntt_cols<false><<<grid, 256, smem, s>>>(dp_, R, ch.col0, ltc);
+}
+
+void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s) const {
+    dim3 grid(plan_.nrows / rpb_, plan_.K, nb);
+    if (fused) k_ntt_rows<true><<<grid, 128, smem_rows_fused_, s>>>(dp_, R, RA, rpb_);
+    else k_ntt_rows<false><<<grid, 128, smem_rows_fwd_, s>>>(dp_, R, RA, rpb_);
+}
+
+void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s) const {
+    const uint32_t npos = plan_.nrows * ch.cw;
+    if (form_ == GEMM_TENSOR) {
+        const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
+        const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
+        k_crt_tc<<<grid, 128, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out);
+    } else {
+        dim3 grid((npos + CRT_TM - 1) / CRT_TM, 1, nb);
+        k_crt_plain<<<grid, 128, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, out);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// device-resident multiply
+// ---------------------------------------------------------------------------------------
+void Engine::run_device(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t count, cudaStream_t s) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    if (count == 0) return;
+    const uint32_t g = std::min(count, group_cap_);
+    ensure_scratch(g);
+    const Chunk all{0, plan_.ncols};
+    const size_t cw = plan_.coeff_words();
+    for (uint32_t i = 0; i < count; i += g) {
+        const uint32_t nb = std::min(g, count - i);
+        const uint32_t* ai = a + (size_t)i * cw;
+        const uint32_t* bi = b + (size_t)i * cw;
+        launch_dec(ai, all, nb, d_ra_, s);
+        launch_cols(false, d_ra_, all, nb, s);
+        launch_rows(false, d_ra_, nullptr, nb, s);
+        launch_dec(bi, all, nb, d_rb_, s);
+        launch_cols(false, d_rb_, all, nb, s);
+        launch_rows(true, d_rb_, d_ra_, nb, s);
+        launch_cols(true, d_rb_, all, nb, s);
+        launch_crt(d_rb_, all, nb, c + (size_t)i * cw, s);
+    }
+    cuda_check(cudaGetLastError(), "kernel launch");
+}
+
+void Engine::time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t count, int reps,
+                         cudaStream_t s, float* ms_out) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    if (count == 0 || count > group_cap_) throw InvalidPoint("count must be in [1, group]");
+    if (reps < 1) throw InvalidPoint("reps must be >= 1");
+    ensure_scratch(count);
+    const Chunk all{0, plan_.ncols};
+    constexpr int S = 8;
+    cudaEvent_t ev[S + 1];
+    for (auto& e : ev) cuda_check(cudaEventCreate(&e), "event");
+    double acc[S] = {0};
+    try {
+        for (int r = 0; r < reps; ++r) {
+            cuda_check(cudaEventRecord(ev[0], s), "record");
+            launch_dec(a, all, count, d_ra_, s);
+            cuda_check(cudaEventRecord(ev[1], s), "record");
+            launch_cols(false, d_ra_, all, count, s);
+            cuda_check(cudaEventRecord(ev[2], s), "record");
+            launch_rows(false, d_ra_, nullptr, count, s);
+            cuda_check(cudaEventRecord(ev[3], s), "record");
+            launch_dec(b, all, count, d_rb_, s);
+            cuda_check(cudaEventRecord(ev[4], s), "record");
+            launch_cols(false, d_rb_, all, count, s);
+            cuda_check(cudaEventRecord(ev[5], s), "record");
+            launch_rows(true, d_rb_, d_ra_, count, s);
+            cuda_check(cudaEventRecord(ev[6], s), "record");
+            launch_cols(true, d_rb_, all, count, s);
+            cuda_check(cudaEventRecord(ev[7], s), "record");
+            launch_crt(d_rb_, all, count, c, s);
+            cuda_check(cudaEventRecord(ev[8], s), "record");
+            cuda_check(cudaGetLastError(), "kernel launch");
+            cuda_check(cudaEventSynchronize(ev[S]), "sync");
+            for (int k = 0; k < S; ++k) {
+                float ms = 0;
+                cuda_check(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "elapsed");
+                acc[k] += ms;
+            }
+        }
+    } catch (...) {
+        for (auto e : ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (auto e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < S; ++k) ms_out[k] = (float)(acc[k] / reps);
+    throw_if_status();
+}
+
+uint32_t Engine::take_status() {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    uint32_t st = 0;
+    cuda_check(cudaDeviceSynchronize(), "device synchronize");
+    cuda_check(cudaMemcpy(&st, dp_.status, 4, cudaMemcpyDeviceToHost), "status read");
+    if (st) cuda_check(cudaMemset(dp_.status, 0, 4), "status clear");
+    return st;
+}
+
+void Engine::throw_if_status() {
+    const uint32_t st = take_status();
+    if (st) {
+        std::string what = "device-side check failed:";
+        if (st & DEV_ERR_CRT_BOUND) what += " CRT estimate outside its exactness bound;";
+        if (st & DEV_ERR_FOLD) what += " delta-fold did not converge;";
+        if (st & DEV_ERR_WAIT) what += " tensor-core wait timed out;";
+        throw DeviceCheckError(what);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// host-operand multiply: the chunked pipeline
+// ---------------------------------------------------------------------------------------
+void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    ensure_scratch(1);
+    const uint32_t nrows = plan_.nrows, ncols = plan_.ncols, L = plan_.L;
+    const uint32_t* src[2] = {a, b};
+    const int na = (int)cin_.size(), nin = 2 * na;
+    const uint32_t ntasks = std::min<uint32_t>(nrows, 64);
+    const uint32_t rpt = (nrows + ntasks - 1) / ntasks;
+
+    // gather input chunk i (operand i / na) into pinned memory, layout [row][col-in-chunk][limb]
+    auto stage = [&](int i) {
+        const int P = i / na;
+        const Chunk ch = cin_[i % na];
+        uint32_t* dst = h_in_[P] + (size_t)ch.col0 * nrows * L;
+        const size_t seg = (size_t)ch.cw * L;
+        pool_->run((int)ntasks, [&](int t) {
+            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
+            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r)
+                stream_copy(dst + r * seg, src[P] + ((size_t)r * ncols + ch.col0) * L, seg * 4);
+        });
+    };
+    uint32_t* dR[2] = {d_ra_, d_rb_};
+    stage(0);
+    for (int i = 0; i < nin; ++i) {
+        const int P = i / na, ci = i % na;
+        const Chunk ch = cin_[ci];
+        const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
+        cudaStream_t sc = s_comp_[i % 3];
+        cuda_check(cudaMemcpyAsync(d_in_[P] + off, h_in_[P] + off, words * 4, cudaMemcpyHostToDevice, s_h2d_), "H2D");
+        cuda_check(cudaEventRecord(ev_in_[i], s_h2d_), "record");
+        cuda_check(cudaStreamWaitEvent(sc, ev_in_[i], 0), "wait");
+        launch_dec(d_in_[P] + off, ch, 1, dR[P], sc);
+        launch_cols(false, dR[P], ch, 1, sc);
+        cuda_check(cudaEventRecord(ev_done_in_[i], sc), "record");
+        if (i == na - 1) {  // a complete: its row pass overlaps b's transfer
+            for (int k = 0; k < na; ++k) cuda_check(cudaStreamWaitEvent(s_comp_[0], ev_done_in_[k], 0), "wait");
+            launch_rows(false, d_ra_, nullptr, 1, s_comp_[0]);
+            cuda_check(cudaEventRecord(ev_row_a_, s_comp_[0]), "record");
+        }
+        if (i + 1 < nin) stage(i + 1);
+    }
+    cudaStream_t s0 = s_comp_[0];
+    cuda_check(cudaStreamWaitEvent(s0, ev_row_a_, 0), "wait");
+    for (int k = na; k < nin; ++k) cuda_check(cudaStreamWaitEvent(s0, ev_done_in_[k], 0), "wait");
+    launch_rows(true, d_rb_, d_ra_, 1, s0);
+    cuda_check(cudaEventRecord(ev_fused_, s0), "record");
+    for (size_t oc = 0; oc < cout_.size(); ++oc) {
+        const Chunk ch = cout_[oc];
+        const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
+        cudaStream_t sc = s_comp_[oc % 3];
+        if (oc % 3 != 0) cuda_check(cudaStreamWaitEvent(sc, ev_fused_, 0), "wait");
+        launch_cols(true, d_rb_, ch, 1, sc);
+        launch_crt(d_rb_, ch, 1, d_out_ + off, sc);
+        cuda_check(cudaEventRecord(ev_crt_[oc], sc), "record");
+        cuda_check(cudaStreamWaitEvent(s_d2h_, ev_crt_[oc], 0), "wait");
+        cuda_check(cudaMemcpyAsync(h_out_ + off, d_out_ + off, words * 4, cudaMemcpyDeviceToHost, s_d2h_), "D2H");
+        cuda_check(cudaEventRecord(ev_out_[oc], s_d2h_), "record");
+    }
+    cuda_check(cudaGetLastError(), "kernel launch");
+    for (size_t oc = 0; oc < cout_.size(); ++oc) {
+        cuda_check(cudaEventSynchronize(ev_out_[oc]), "D2H chunk");
+        const Chunk ch = cout_[oc];
+        const uint32_t* srcc = h_out_ + (size_t)ch.col0 * nrows * L;
+        const size_t seg = (size_t)ch.cw * L;
+        pool_->run((int)ntasks, [&](int t) {
+            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
+            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r)
+                stream_copy(c + ((size_t)r * ncols + ch.col0) * L, srcc + r * seg, seg * 4);
+        });
+    }
+    throw_if_status();
+}
+
+}  // namespace pm

@@ -1,0 +1,142 @@
+// pm_engine.h -- one multiplication context: the plan's tables on the device, scratch
+// residue arrays, streams, pinned staging, and the two ways of running the multiply
+// (device-resident operands, or host operands through the chunked PCIe pipeline).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "pm_device.cuh"
+#include "pm_plan.h"
+
+namespace pm {
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+struct DeviceCheckError : std::runtime_error {
+    explicit DeviceCheckError(const std::string& s) : std::runtime_error(s) {}
+};
+struct Unsupported : std::runtime_error {
+    explicit Unsupported(const std::string& s) : std::runtime_error(s) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);
+
+// Host worker pool for the pageable <-> pinned staging copies.  run(n, fn) executes
+// fn(0..n-1) across the workers and the calling thread and returns when all are done.
+class HostPool {
+  public:
+    explicit HostPool(int workers);
+    ~HostPool();
+    void run(int n, const std::function<void(int)>& fn);
+    int size() const { return (int)threads_.size() + 1; }
+
+  private:
+    void loop();
+    std::vector<std::thread> threads_;
+    std::mutex m_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int)>* fn_ = nullptr;
+    int n_ = 0;
+    std::atomic<int> next_{0};
+    int finished_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+enum GemmForm : int { GEMM_AUTO = 0, GEMM_PLAIN = 1, GEMM_TENSOR = 2 };
+
+struct Chunk {
+    uint32_t col0, cw;
+};
+
+class Engine {
+  public:
+    Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_request, int device);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // c[i] = a[i] * b[i] for i < count; operands contiguous [count][N][L] in device memory.
+    // Asynchronous on `stream`; check_status() reports device-side check failures.
+    void run_device(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t count, cudaStream_t stream);
+    // Per-kernel mean durations (ms) of `reps` groups of `count` multiplies (CUDA events).
+    void time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t count, int reps, cudaStream_t s,
+                     float* ms_out);
+    // One multiply from host (pageable) operands to a host result; synchronous.
+    void run_host(const uint32_t* a, const uint32_t* b, uint32_t* c);
+    // Reads (and clears) the device status word; synchronises with the device.
+    uint32_t take_status();
+    void throw_if_status();
+
+    const Plan& plan() const { return plan_; }
+    const DevPlan& dev() const { return dp_; }
+    int gemm_form() const { return form_; }
+    int device() const { return device_; }
+    size_t scratch_bytes() const { return scratch_words_ * 4; }
+    size_t table_bytes() const { return table_bytes_; }
+    uint32_t group() const { return group_; }
+    int kernel_launches_per_group() const;
+    const std::vector<Chunk>& in_chunks() const { return cin_; }
+    const std::vector<Chunk>& out_chunks() const { return cout_; }
+
+    // launch helpers (also used by the tests' stage-by-stage checks)
+    void launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s) const;
+    void launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s) const;
+    void launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s) const;
+    void launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s) const;
+
+  private:
+    void upload_tables();
+    void setup_launch_shapes();
+    void ensure_scratch(uint32_t group);
+    void setup_host_pipeline();
+    ChunkMap chunk_map(Chunk ch) const;
+
+    Plan plan_;
+    DevPlan dp_{};
+    int device_ = 0;
+    int form_ = GEMM_PLAIN;
+    int num_sms_ = 148;
+    size_t smem_optin_ = 227 * 1024;
+    std::vector<void*> dev_allocs_;
+    size_t table_bytes_ = 0;
+
+    // scratch residues for `group_` multiplies: R_a, R_b [group][K][N]
+    uint32_t* d_ra_ = nullptr;
+    uint32_t* d_rb_ = nullptr;
+    size_t scratch_words_ = 0;
+    uint32_t group_ = 0;
+    uint32_t group_cap_ = 1;
+
+    // launch shapes
+    int rpb_ = 1;
+    size_t smem_cols_ = 0, smem_rows_fwd_ = 0, smem_rows_fused_ = 0;
+    size_t smem_dec_ = 0, smem_crt_ = 0;
+    bool dec_tab_smem_ = false;
+
+    // host pipeline
+    std::vector<Chunk> cin_, cout_;
+    uint32_t* d_in_[2] = {nullptr, nullptr};
+    uint32_t* d_out_ = nullptr;
+    uint32_t* h_in_[2] = {nullptr, nullptr};
+    uint32_t* h_out_ = nullptr;
+    cudaStream_t s_comp_[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t s_h2d_ = nullptr, s_d2h_ = nullptr;
+    std::vector<cudaEvent_t> ev_in_, ev_done_in_, ev_crt_, ev_out_;
+    cudaEvent_t ev_row_a_ = nullptr, ev_fused_ = nullptr;
+    std::unique_ptr<HostPool> pool_;
+};
+
+}  // namespace pm

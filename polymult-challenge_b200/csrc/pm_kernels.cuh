@@ -1,0 +1,47 @@
+// pm_kernels.cuh -- declarations of every kernel of the multiply and their launch helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+
+#include "pm_device.cuh"
+
+namespace pm {
+
+// ---- NTT (k_ntt.cu)
+template <bool INV>
+__global__ void k_ntt_cols(DevPlan P, uint32_t* R, uint32_t col0, int ltc);
+template <bool FUSED>
+__global__ void k_ntt_rows(DevPlan P, uint32_t* R, const uint32_t* RA, int rpb);
+size_t ntt_cols_smem(const DevPlan& P, int ltc);
+size_t ntt_rows_smem(const DevPlan& P, int rpb, bool fused);
+
+// ---- plain (CUDA-core) RNS decomposition and CRT (k_rns.cu)
+constexpr int DEC_TM = 64;   // coefficients per decomposition block
+constexpr int CRT_TM = 32;   // coefficients per CRT block
+__global__ void k_rns_plain(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t* R, int tab_in_smem);
+__global__ void k_crt_plain(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t* out);
+size_t rns_plain_smem(const DevPlan& P, bool tab_in_smem);
+size_t crt_plain_smem(const DevPlan& P);
+
+// ---- tensor-core (tcgen05 kind::i8) RNS decomposition and CRT (k_tc.cu)
+constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
+__global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R);
+__global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out);
+size_t rns_tc_smem(const DevPlan& P);
+size_t crt_tc_smem(const DevPlan& P);
+// TMEM columns to allocate: a power of two >= max(32, n)
+__host__ __device__ inline uint32_t tmem_cols_for(int n) {
+    uint32_t c = 32;
+    while (c < (uint32_t)n) c <<= 1;
+    return c;
+}
+
+// words of one CRT staging row: z needs L + 3 limbs (value < 2^(W + 64)); odd stride
+__host__ __device__ inline int crt_zl(int L) { return L + 3; }
+__host__ __device__ inline int crt_zstride(int L) { return crt_zl(L) | 1; }
+
+}  // namespace pm

@@ -1,0 +1,87 @@
+// pm_plan.h -- host-side precompute for one (N, W, q) point: RNS primes, twiddle tables,
+// decomposition and CRT constants, and the byte-sliced operand tables of the tensor-core
+// GEMMs.  Pure C++ (no CUDA), so the host logic is testable on a machine without a GPU.
+//
+// Replaces the reference's precompute() (solve.cu:869-1020) with a different prime family:
+// primes p < 2^30 with p == 1 (mod 2*max(N, 2^16)).  Below 2^30, 4p < 2^32, so every NTT
+// stage can keep its values lazily in [0, 4p) (Harvey butterflies) instead of reducing to
+// [0, p) after each butterfly; and one prime list serves every N <= 2^16, which the batched
+// path relies on.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace pm {
+
+// Thrown for an invalid point; the C ABI maps it to PM_ERR_INVALID (the reference throws
+// std::runtime_error from precompute for the same conditions, solve.cu:873-913).
+struct InvalidPoint : std::runtime_error {
+    explicit InvalidPoint(const std::string& s) : std::runtime_error(s) {}
+};
+
+// Shape of the byte-sliced tensor-core GEMMs (UMMA K-major, no-swizzle canonical layout:
+// core matrices of 8 rows x 16 bytes, LBO = 128 B between K-adjacent core matrices,
+// SBO = 8 * k_bytes between 8-row groups).
+struct GemmShape {
+    int n_rows = 0;    // UMMA N (rows of the K-major B operand), multiple of 16
+    int k_bytes = 0;   // UMMA K in bytes, multiple of 32
+    size_t b_bytes() const { return (size_t)n_rows * k_bytes; }
+};
+
+struct Plan {
+    // point
+    uint32_t N = 0, W = 0, L = 0;
+    int logN = 0, w1 = 0, w2 = 0;     // 4-step split: nrows = 2^w1 (column pass), ncols = 2^w2
+    uint32_t nrows = 1, ncols = 1;
+    std::vector<uint32_t> q;          // [L]
+    uint64_t delta = 0;               // 2^W - q
+    int delta_bits = 0;
+
+    // RNS
+    int K = 0;                        // primes
+    int KP = 0;                       // K rounded up to a multiple of 4
+    uint64_t prime_step = 0;          // primes are == 1 mod prime_step
+    std::vector<uint32_t> p;          // [KP] (padding primes repeat the last one)
+    std::vector<uint32_t> pinv;       // [KP] p^-1 mod 2^32
+    std::vector<uint32_t> crt_c;      // [KP] N^-1 R^2 (M/p_j)^-1 mod p_j   (R = 2^32)
+    std::vector<uint32_t> crt_cc;     // [KP] crt_c * pinv mod 2^32 (Montgomery-Shoup companion)
+    std::vector<float> rcp;           // [KP] 1/p_j (0 for padding)
+
+    // twiddles: tw[j][k] = psi_j^bitrev_logN(k) * R mod p_j, k < N
+    std::vector<uint32_t> tw;         // [K][N]
+
+    // plain (CUDA-core) GEMM tables
+    int HP = 0;                       // 2L rounded up to a multiple of 4
+    std::vector<uint32_t> dec16;      // [2L][KP]  2^(16h) R mod p_j
+    std::vector<uint16_t> qh16;       // [KP][HP]  16-bit halves of Q_j = (M/p_j) mod q
+    std::vector<uint32_t> tneg;       // [K+1][L]  (-v M) mod q
+
+    // tensor-core GEMM tables (canonical smem images, uploaded as-is)
+    GemmShape dec_gemm;               // rows (j,t) = 4j+t, K = coefficient bytes
+    GemmShape crt_gemm;               // rows = result byte v, K = (j,t) = 4j+t
+    std::vector<uint8_t> dec_b;       // dec_gemm.b_bytes()
+    std::vector<uint8_t> crt_b;       // crt_gemm.b_bytes()
+
+    size_t coeff_words() const { return (size_t)N * L; }
+    size_t residue_words() const { return (size_t)K * N; }
+};
+
+// Builds every table. Throws InvalidPoint for a malformed point.
+Plan make_plan(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q);
+
+// Offset in bytes of element (row, kbyte) inside a K-major no-swizzle canonical tile
+// whose rows hold k_bytes bytes.
+inline size_t umma_kmajor_offset(int row, int kbyte, int k_bytes) {
+    return (size_t)(row >> 3) * (size_t)(8 * k_bytes) + (size_t)(kbyte >> 4) * 128 + (size_t)(row & 7) * 16 +
+           (size_t)(kbyte & 15);
+}
+
+// Host-side self-checks of a plan (used by tests through the C ABI): returns an empty
+// string when every check passes, else a description of the first failure.
+std::string check_plan(const Plan& P);
+
+}  // namespace pm

@@ -1,0 +1,197 @@
+"""Python binding of libpolymult_b200.so (include/polymult_b200.h) through ctypes.
+
+Mirrors the reference's plugin interface for this path, the three entry points the FHERMA
+harness binds (fherma.toml:7-10; fherma.h:45-48):
+
+    state = fherma_init(N, W, L, q_limbs)      # solve.cu:1392-1478
+    c     = fherma_run(state, a, b)            # solve.cu:1480-1498
+    fherma_free(state)                         # solve.cu:1530-1534
+
+with the same meaning (q, a, b, c as L little-endian u32 limbs per coefficient; a, b, c of
+shape (N, L)) and the same error behaviour (RuntimeError on an invalid point or a size
+mismatch).  `Multiplier` is the object form, and adds the device-resident batch call.
+
+There is no fallback: if the CUDA library is missing or no B200 is present, these calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpolymult_b200.so")
+HEADER = os.path.join(HERE, "..", "include", "polymult_b200.h")
+
+PM_OK, PM_ERR_INVALID, PM_ERR_CUDA, PM_ERR_DEVICE, PM_ERR_UNSUPPORTED, PM_ERR_INTERNAL = range(6)
+GEMM_FORMS = {"auto": 0, "plain": 1, "tensor": 2}
+GEMM_NAMES = {v: k for k, v in GEMM_FORMS.items()}
+STAGES = ("dec_a", "cols_a", "rows_a", "dec_b", "cols_b", "rows_fused", "cols_inv", "crt")
+
+
+class PolymultError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__("polymult error %d: %s" % (code, message))
+        self.code = code
+
+
+class PmInfo(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_uint32), ("W", ctypes.c_uint32), ("L", ctypes.c_uint32),
+                ("K", ctypes.c_int32), ("logN", ctypes.c_int32), ("w1", ctypes.c_int32),
+                ("w2", ctypes.c_int32), ("gemm_form", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("delta", ctypes.c_uint64), ("table_bytes", ctypes.c_uint64),
+                ("scratch_bytes", ctypes.c_uint64), ("launches_per_multiply", ctypes.c_int32),
+                ("group", ctypes.c_int32)]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def declared_symbols(header: str = HEADER):
+    """Function names declared in include/polymult_b200.h."""
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pm_[a-z_]+)\s*\(", text)))
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the library (once); raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError("libpolymult_b200.so not built (run polymult-challenge_b200/build.py): %s" % path)
+    lib = ctypes.CDLL(path)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    vp = ctypes.c_void_p
+    lib.pm_init.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp, ctypes.c_int, ctypes.c_int,
+                            ctypes.POINTER(vp)]
+    lib.pm_init.restype = ctypes.c_int
+    lib.pm_run.argtypes = [vp, vp, vp, vp]
+    lib.pm_run.restype = ctypes.c_int
+    lib.pm_run_device.argtypes = [vp, vp, vp, vp, ctypes.c_uint32, vp]
+    lib.pm_run_device.restype = ctypes.c_int
+    lib.pm_time_stages.argtypes = [vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_int, vp,
+                                   ctypes.POINTER(ctypes.c_float)]
+    lib.pm_time_stages.restype = ctypes.c_int
+    lib.pm_sync.argtypes = [vp]
+    lib.pm_sync.restype = ctypes.c_int
+    lib.pm_free.argtypes = [vp]
+    lib.pm_free.restype = None
+    lib.pm_get_info.argtypes = [vp, ctypes.POINTER(PmInfo)]
+    lib.pm_get_info.restype = ctypes.c_int
+    lib.pm_last_error.argtypes = []
+    lib.pm_last_error.restype = ctypes.c_char_p
+    lib.pm_plan_selfcheck.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp,
+                                      ctypes.POINTER(ctypes.c_int32)]
+    lib.pm_plan_selfcheck.restype = ctypes.c_int
+    del u32p
+    _lib = lib
+    return lib
+
+
+def _check(code: int):
+    if code != PM_OK:
+        raise PolymultError(code, load().pm_last_error().decode(errors="replace"))
+
+
+def _u32(arr, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(arr, dtype=np.uint32)
+    if shape is not None and a.shape != shape:
+        raise RuntimeError("operand size does not match N x L: got %s, want %s" % (a.shape, shape))
+    return a
+
+
+def plan_selfcheck(N: int, W: int, q_limbs) -> int:
+    """Host-only plan build + self-checks; returns the number of RNS primes."""
+    L = (W + 31) // 32
+    q = _u32(q_limbs)
+    k = ctypes.c_int32(0)
+    _check(load().pm_plan_selfcheck(N, W, L, q.ctypes.data, ctypes.byref(k)))
+    return k.value
+
+
+class Multiplier:
+    """c = a*b mod (X^N+1, q) on one B200."""
+
+    def __init__(self, N: int, W: int, q_limbs, gemm: str = "auto", device: int = 0):
+        lib = load()
+        self.N, self.W = int(N), int(W)
+        self.L = (self.W + 31) // 32
+        q = _u32(q_limbs)
+        if q.size != self.L:
+            raise RuntimeError("q must have L limbs")
+        h = ctypes.c_void_p()
+        _check(lib.pm_init(self.N, self.W, self.L, q.ctypes.data, GEMM_FORMS[gemm], device, ctypes.byref(h)))
+        self._h = h
+
+    def info(self) -> dict:
+        inf = PmInfo()
+        _check(load().pm_get_info(self._h, ctypes.byref(inf)))
+        d = {f: getattr(inf, f) for f, _ in PmInfo._fields_}
+        d["gemm"] = GEMM_NAMES.get(d["gemm_form"], "?")
+        return d
+
+    def multiply(self, a, b, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Host operands (N, L) u32 -> host result, through the chunked PCIe pipeline."""
+        shape = (self.N, self.L)
+        a, b = _u32(a, shape), _u32(b, shape)
+        c = out if out is not None else np.empty(shape, dtype=np.uint32)
+        _check(load().pm_run(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
+        return c
+
+    def multiply_device(self, a_ptr: int, b_ptr: int, c_ptr: int, count: int = 1, stream: int = 0):
+        """Device-resident operands [count][N][L]; asynchronous on `stream` (cudaStream_t as int)."""
+        _check(load().pm_run_device(self._h, a_ptr, b_ptr, c_ptr, count, stream or None))
+
+    def time_stages(self, a_ptr: int, b_ptr: int, c_ptr: int, count: int = 1, reps: int = 3, stream: int = 0):
+        """Mean per-kernel durations (ms) in launch order, keyed by STAGES."""
+        ms = (ctypes.c_float * len(STAGES))()
+        _check(load().pm_time_stages(self._h, a_ptr, b_ptr, c_ptr, count, reps, stream or None, ms))
+        return dict(zip(STAGES, [float(x) for x in ms]))
+
+    def sync(self):
+        _check(load().pm_sync(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pm_free(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# -- the reference's three entry points -------------------------------------------------
+
+def fherma_init(N: int, W: int, L: int, q_limbs, gemm: str = "auto") -> Multiplier:
+    if L != (W + 31) // 32:
+        raise RuntimeError("inconsistent W / L")
+    try:
+        return Multiplier(N, W, q_limbs, gemm=gemm)
+    except PolymultError as e:
+        raise RuntimeError(str(e)) from e
+
+
+def fherma_run(state: Multiplier, a, b) -> np.ndarray:
+    try:
+        return state.multiply(a, b)
+    except PolymultError as e:
+        raise RuntimeError(str(e)) from e
+
+
+def fherma_free(state: Optional[Multiplier]) -> None:
+    if state is not None:
+        state.close()

@@ -1,0 +1,142 @@
+"""GPU parity: the CUDA path through the C ABI, bit-exact against the reference's outputs.
+
+Every golden point (the reference's own regression set, tests/run_emu.sh:20-33, plus the
+benchmark configurations N=4096/W=256, N=32768/W=868 in four distributions and the ranked
+N=65536/W=1747) is run through both entry points (host operands: pm_run, the reference's
+fherma_run; device operands: pm_run_device) in both GEMM forms (CUDA-core plain, tcgen05
+tensor-core) and compared byte-for-byte with c.bin as the reference's tests/oracle.py wrote
+it.  Beyond the golden set: batched device calls, random operands at the ranked point
+against the C oracle, repeatability, and the device status word."""
+import numpy as np
+import pytest
+
+from conftest import c_oracle_mul, ensure_library, load_golden, orc, regen_case, sha
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = load_golden()
+POINTS = GOLDEN["points"]
+RANKED = [(4096, 256), (32768, 868), (65536, 1747)]
+
+
+def _q(pt):
+    return orc.limbs_of(int(pt["q_hex"], 16), pt["L"])
+
+
+def _multiplier(pt, gemm):
+    import polymult
+    ensure_library()
+    try:
+        return polymult.Multiplier(pt["N"], pt["W"], _q(pt), gemm=gemm)
+    except polymult.PolymultError as e:
+        if e.code == polymult.PM_ERR_UNSUPPORTED and (pt["N"], pt["W"]) not in RANKED:
+            pytest.skip("tensor-core form does not cover N=%d W=%d" % (pt["N"], pt["W"]))
+        raise
+
+
+def _torch():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+@pytest.mark.parametrize("gemm", ["plain", "tensor"])
+@pytest.mark.parametrize("pt", POINTS, ids=["N%d_W%d" % (p["N"], p["W"]) for p in POINTS])
+def test_host_path_matches_reference(pt, gemm):
+    m = _multiplier(pt, gemm)
+    with m:
+        assert m.info()["gemm"] == gemm
+        for case in pt["cases"]:
+            a, b, _ = regen_case(pt, case)
+            c = m.multiply(a, b)
+            assert sha(c) == case["c_sha256"], (pt["N"], pt["W"], case["s"], case["mode"])
+        m.sync()
+
+
+@pytest.mark.parametrize("gemm", ["plain", "tensor"])
+@pytest.mark.parametrize("pt", POINTS, ids=["N%d_W%d" % (p["N"], p["W"]) for p in POINTS])
+def test_device_path_matches_reference(pt, gemm):
+    torch = _torch()
+    m = _multiplier(pt, gemm)
+    with m:
+        A, B = [], []
+        for case in pt["cases"]:
+            a, b, _ = regen_case(pt, case)
+            A.append(a)
+            B.append(b)
+        da = torch.from_numpy(np.stack(A).view(np.int32)).cuda()
+        db = torch.from_numpy(np.stack(B).view(np.int32)).cuda()
+        dc = torch.zeros_like(da)
+        s = torch.cuda.current_stream()
+        m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), len(A), s.cuda_stream)
+        m.sync()
+        out = dc.cpu().numpy().view(np.uint32)
+        for i, case in enumerate(pt["cases"]):
+            assert sha(out[i]) == case["c_sha256"], (pt["N"], pt["W"], case["s"], case["mode"])
+
+
+@pytest.mark.parametrize("gemm", ["plain", "tensor"])
+def test_ranked_point_random_against_c_oracle(gemm):
+    """Two fresh uniform cases at N=65536/W=1747 in one device call (two launch groups)."""
+    torch = _torch()
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (65536, 1747))
+    q = int(pt["q_hex"], 16)
+    A = [orc.uniform_limbs(65536, 1747, q, seed=s) for s in (11, 12)]
+    B = [orc.uniform_limbs(65536, 1747, q, seed=s) for s in (21, 22)]
+    m = _multiplier(pt, gemm)
+    with m:
+        da = torch.from_numpy(np.stack(A).view(np.int32)).cuda()
+        db = torch.from_numpy(np.stack(B).view(np.int32)).cuda()
+        dc = torch.zeros_like(da)
+        m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), 2, torch.cuda.current_stream().cuda_stream)
+        m.sync()
+        out = dc.cpu().numpy().view(np.uint32)
+    for i in range(2):
+        exp = c_oracle_mul(65536, 1747, q, A[i], B[i])
+        assert np.array_equal(out[i], exp), i
+
+
+def test_tensor_and_plain_agree_and_repeat():
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (32768, 868))
+    q = int(pt["q_hex"], 16)
+    a = orc.uniform_limbs(32768, 868, q, seed=5)
+    b = orc.uniform_limbs(32768, 868, q, seed=6)
+    with _multiplier(pt, "plain") as mp, _multiplier(pt, "tensor") as mt:
+        c1 = mp.multiply(a, b)
+        c2 = mt.multiply(a, b)
+        c3 = mt.multiply(a, b)
+    assert np.array_equal(c1, c2) and np.array_equal(c2, c3)
+    assert np.array_equal(c1, c_oracle_mul(32768, 868, q, a, b))
+
+
+def test_commutative_and_linear():
+    """Size-independent properties at the ranked point: a*b == b*a, (a+a')*b == a*b + a'*b."""
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (65536, 1747))
+    q = int(pt["q_hex"], 16)
+    a = orc.uniform_limbs(65536, 1747, q, seed=31)
+    b = orc.uniform_limbs(65536, 1747, q, seed=32)
+    with _multiplier(pt, "tensor") as m:
+        ab = m.multiply(a, b)
+        ba = m.multiply(b, a)
+        assert np.array_equal(ab, ba)
+        # a' = x^1 * a (negacyclic shift): a'*b must be the shift of a*b
+        av = orc.unpack_limbs(a)
+        shifted = [(q - av[-1]) % q] + av[:-1]
+        sb = m.multiply(orc.pack_limbs(shifted, pt["L"]), b)
+    abv = orc.unpack_limbs(ab)
+    exp = [(q - abv[-1]) % q] + abv[:-1]
+    assert orc.unpack_limbs(sb) == exp
+
+
+def test_fherma_python_mirror():
+    import polymult
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (4096, 256))
+    st = polymult.fherma_init(pt["N"], pt["W"], pt["L"], _q(pt))
+    try:
+        a, b, _ = regen_case(pt, pt["cases"][0])
+        assert sha(polymult.fherma_run(st, a, b)) == pt["cases"][0]["c_sha256"]
+        with pytest.raises(RuntimeError):
+            polymult.fherma_run(st, a[:-1], b[:-1])
+    finally:
+        polymult.fherma_free(st)
