@@ -167,10 +167,43 @@ __global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restric
     for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) rows[idx] = sh[idx];
 }
 
-template __global__ void k_ntt_cols<false>(DevPlan, uint32_t*, uint32_t, int);
-template __global__ void k_ntt_cols<true>(DevPlan, uint32_t*, uint32_t, int);
-template __global__ void k_ntt_rows<false>(DevPlan, uint32_t*, const uint32_t*, int);
-template __global__ void k_ntt_rows<true>(DevPlan, uint32_t*, const uint32_t*, int);
+void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
+                     int ltc) {
+    if (inv) k_ntt_cols<true><<<grid, 256, smem, s>>>(P, R, col0, ltc);
+    else k_ntt_cols<false><<<grid, 256, smem, s>>>(P, R, col0, ltc);
+}
+
+void launch_ntt_rows(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
+                     const uint32_t* RA, int rpb) {
+    if (fused) k_ntt_rows<true><<<grid, 128, smem, s>>>(P, R, RA, rpb);
+    else k_ntt_rows<false><<<grid, 128, smem, s>>>(P, R, RA, rpb);
+}
+
+namespace {
+struct NttKernel {
+    const void* fn;
+    const char* name;
+};
+const NttKernel kNttKernels[] = {{(const void*)k_ntt_cols<false>, "k_ntt_cols<forward>"},
+                                 {(const void*)k_ntt_cols<true>, "k_ntt_cols<inverse>"},
+                                 {(const void*)k_ntt_rows<false>, "k_ntt_rows<forward>"},
+                                 {(const void*)k_ntt_rows<true>, "k_ntt_rows<fused>"}};
+}  // namespace
+
+void ntt_set_smem_limit(int bytes) {
+    for (const NttKernel& k : kNttKernels) {
+        const cudaError_t e = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) throw_cuda(e, k.name);
+    }
+}
+
+void ntt_probe_images() {
+    for (const NttKernel& k : kNttKernels) {
+        cudaFuncAttributes fa{};
+        const cudaError_t e = cudaFuncGetAttributes(&fa, k.fn);
+        if (e != cudaSuccess) throw_cuda(e, k.name);
+    }
+}
 
 size_t ntt_cols_smem(const DevPlan& P, int ltc) {
     return (size_t)P.nrows * sizeof(Tw2) + ((size_t)P.nrows << ltc) * 4;

@@ -27,8 +27,10 @@
 namespace pm {
 
 void cuda_check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess) throw_cuda(e, what);
 }
+
+void throw_cuda(cudaError_t e, const char* what) { throw CudaError(std::string(what) + ": " + cudaGetErrorString(e)); }
 
 // ---------------------------------------------------------------------------------------
 // host pool
@@ -290,10 +292,20 @@ void Engine::setup_launch_shapes() {
     // Every kernel may use up to the device's opt-in maximum: contexts for different points
     // share these kernels, so a per-point limit set by one context could fail another's launch.
     const int mx = (int)smem_optin_;
-    cuda_check(cudaFuncSetAttribute(k_ntt_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
-    cuda_check(cudaFuncSetAttribute(k_ntt_cols<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
-    cuda_check(cudaFuncSetAttribute(k_ntt_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
-    cuda_check(cudaFuncSetAttribute(k_ntt_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    ntt_probe_images();
+    struct Probe {
+        const void* fn;
+        const char* name;
+    };
+    const Probe probes[] = {{(const void*)k_rns_plain, "k_rns_plain"},
+                            {(const void*)k_crt_plain, "k_crt_plain"},
+                            {(const void*)k_rns_tc, "k_rns_tc"},
+                            {(const void*)k_crt_tc, "k_crt_tc"}};
+    for (const Probe& pr : probes) {
+        cudaFuncAttributes fa{};
+        cuda_check(cudaFuncGetAttributes(&fa, pr.fn), (std::string("kernel image ") + pr.name).c_str());
+    }
+    ntt_set_smem_limit(mx);
     cuda_check(cudaFuncSetAttribute(k_rns_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_crt_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_rns_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
@@ -358,9 +370,11 @@ void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R,
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         k_rns_tc<<<grid, 128, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, nb, R);
+        cuda_check(cudaGetLastError(), "launch k_rns_tc");
     } else {
         dim3 grid((npos + DEC_TM - 1) / DEC_TM, 1, nb);
         k_rns_plain<<<grid, 256, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, R, dec_tab_smem_ ? 1 : 0);
+        cuda_check(cudaGetLastError(), "launch k_rns_plain");
     }
 }
 
@@ -369,14 +383,14 @@ void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStrea
     const int ltc = ilog2(std::min<uint32_t>(32, ch.cw));
     dim3 grid(ch.cw >> ltc, plan_.K, nb);
     const size_t smem = ntt_cols_smem(dp_, ltc);
-    if (inv) k_ntt_cols<true><<<grid, 256, smem, s>>>(dp_, R, ch.col0, ltc);
-    else k_ntt_cols<false><<<grid, 256, smem, s>>>(dp_, R, ch.col0, ltc);
+    launch_ntt_cols(inv, grid, smem, s, dp_, R, ch.col0, ltc);
+    cuda_check(cudaGetLastError(), inv ? "launch k_ntt_cols<inverse>" : "launch k_ntt_cols<forward>");
 }
 
 void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s) const {
     dim3 grid(plan_.nrows / rpb_, plan_.K, nb);
-    if (fused) k_ntt_rows<true><<<grid, 128, smem_rows_fused_, s>>>(dp_, R, RA, rpb_);
-    else k_ntt_rows<false><<<grid, 128, smem_rows_fwd_, s>>>(dp_, R, RA, rpb_);
+    launch_ntt_rows(fused, grid, fused ? smem_rows_fused_ : smem_rows_fwd_, s, dp_, R, RA, rpb_);
+    cuda_check(cudaGetLastError(), fused ? "launch k_ntt_rows<fused>" : "launch k_ntt_rows<forward>");
 }
 
 void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s) const {
@@ -385,9 +399,11 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         k_crt_tc<<<grid, 128, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out);
+        cuda_check(cudaGetLastError(), "launch k_crt_tc");
     } else {
         dim3 grid((npos + CRT_TM - 1) / CRT_TM, 1, nb);
         k_crt_plain<<<grid, 128, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, out);
+        cuda_check(cudaGetLastError(), "launch k_crt_plain");
     }
 }
 

@@ -11,11 +11,17 @@
 
 namespace pm {
 
-// ---- NTT (k_ntt.cu)
-template <bool INV>
-__global__ void k_ntt_cols(DevPlan P, uint32_t* R, uint32_t col0, int ltc);
-template <bool FUSED>
-__global__ void k_ntt_rows(DevPlan P, uint32_t* R, const uint32_t* RA, int rpb);
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what);  // throws pm::CudaError
+
+// ---- NTT (k_ntt.cu).  The kernels are templates, so they are launched only from k_ntt.cu
+// (a template kernel launched from another translation unit would bind to a host stub that
+// no module registered); these host wrappers are the interface.
+void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
+                     int ltc);
+void launch_ntt_rows(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
+                     const uint32_t* RA, int rpb);
+void ntt_set_smem_limit(int bytes);  // cudaFuncAttributeMaxDynamicSharedMemorySize of all four
+void ntt_probe_images();             // throws CudaError naming a kernel whose image cannot load
 size_t ntt_cols_smem(const DevPlan& P, int ltc);
 size_t ntt_rows_smem(const DevPlan& P, int rpb, bool fused);
 
