@@ -12,24 +12,26 @@
 //     butterfly (solve.cu:286-338);
 //   * column tiles are 32 columns wide (128-byte row segments) so that a warp reads whole
 //     lines and its 32 lanes hit 32 different banks.
+#include <type_traits>
+
 #include "pm_kernels.cuh"
 
 namespace pm {
 namespace {
 
-// Radix-2^RAD group g of a pass starting at local stage ls0 on a line of 2^nb elements at
-// element stride es.  Its elements are idx_e = (hi << (nb - ls0)) | (e << sub) | lo with
-// sub = nb - ls0 - RAD, lo = g mod 2^sub, hi = g >> sub.  Local stage ls0 + k pairs e and
-// e + 2^(RAD-1-k); the twiddle argument (the stage's group index within the line) is
-// (hi << k) | (e >> (RAD - k)).  twf(ls, gi) returns the (already mirrored, for INV) twiddle.
-template <int RAD, bool INV, class TwF>
-__device__ __forceinline__ void radix_group(uint32_t* line, int es, int nb, int ls0, int g, const TwF& twf,
-                                            uint32_t p) {
+// Radix-2^RAD group g of the pass that starts at local stage LS0 of a line of 2^NB elements
+// at element stride es (all shapes compile-time except the stride).  The group's elements are
+// idx_e = (hi << (NB - LS0)) | (e << SUB) | lo with SUB = NB - LS0 - RAD, lo = g mod 2^SUB,
+// hi = g >> SUB.  Local stage LS0 + k pairs e and e + 2^(RAD-1-k); the twiddle argument (the
+// stage's group index within the line) is (hi << k) | (e >> (RAD - k)).  twf(ls, gi) returns
+// the twiddle (for INV, already the mirrored one).
+template <int NB, int LS0, int RAD, bool INV, class TwF>
+__device__ __forceinline__ void radix_group(uint32_t* line, int es, int g, const TwF& twf, uint32_t p) {
     constexpr int G = 1 << RAD;
-    const int sub = nb - ls0 - RAD;
-    const int lo = g & ((1 << sub) - 1), hi = g >> sub;
-    uint32_t* b = line + (size_t)((hi << (nb - ls0)) | lo) * es;
-    const int step = es << sub;
+    constexpr int SUB = NB - LS0 - RAD;
+    const int lo = g & ((1 << SUB) - 1), hi = g >> SUB;
+    uint32_t* b = line + ((hi << (NB - LS0)) | lo) * es;
+    const int step = es << SUB;
     uint32_t v[G];
 #pragma unroll
     for (int e = 0; e < G; ++e) v[e] = b[e * step];
@@ -39,7 +41,7 @@ __device__ __forceinline__ void radix_group(uint32_t* line, int es, int nb, int 
             const int h = G >> (k + 1);
 #pragma unroll
             for (int m = 0; m < (1 << k); ++m) {
-                const Tw2 w = twf(ls0 + k, (hi << k) | m);
+                const Tw2 w = twf(LS0 + k, (hi << k) | m);
 #pragma unroll
                 for (int i = 0; i < h; ++i) bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
             }
@@ -50,7 +52,7 @@ __device__ __forceinline__ void radix_group(uint32_t* line, int es, int nb, int 
             const int h = G >> (k + 1);
 #pragma unroll
             for (int m = 0; m < (1 << k); ++m) {
-                const Tw2 w = twf(ls0 + k, (hi << k) | m);
+                const Tw2 w = twf(LS0 + k, (hi << k) | m);
 #pragma unroll
                 for (int i = 0; i < h; ++i) bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
             }
@@ -60,45 +62,141 @@ __device__ __forceinline__ void radix_group(uint32_t* line, int es, int nb, int 
     for (int e = 0; e < G; ++e) b[e * step] = v[e];
 }
 
-template <bool INV, class TwF>
-__device__ __forceinline__ void radix_group_r(int r, uint32_t* line, int es, int nb, int ls0, int g, const TwF& twf,
-                                              uint32_t p) {
-    if (r == 3) radix_group<3, INV>(line, es, nb, ls0, g, twf, p);
-    else if (r == 2) radix_group<2, INV>(line, es, nb, ls0, g, twf, p);
-    else radix_group<1, INV>(line, es, nb, ls0, g, twf, p);
+template <int V>
+using IntC = std::integral_constant<int, V>;
+
+// Runs body(IntC<LS0>, IntC<RAD>) for every radix-8 pass of a 2^NB-point line transform
+// (forward: LS0 = 0, 3, 6, ...; inverse: the same passes in reverse), one barrier after each.
+template <int NB, int PI, bool INV, class Body>
+__device__ __forceinline__ void for_each_pass(const Body& body) {
+    constexpr int NPASS = (NB + 2) / 3;
+    if constexpr (PI < NPASS) {
+        constexpr int IDX = INV ? NPASS - 1 - PI : PI;
+        constexpr int LS0 = 3 * IDX;
+        constexpr int RAD = (NB - LS0) < 3 ? (NB - LS0) : 3;
+        body(IntC<LS0>{}, IntC<RAD>{});
+        __syncthreads();
+        for_each_pass<NB, PI + 1, INV>(body);
+    }
+}
+
+// Copies a tile of `rows` x `tc` words between global (row stride gstride) and shared
+// (dense [rows][tc]); with 16-byte vectors, eight loads in flight per thread before any store.
+template <bool TO_SMEM>
+__device__ __forceinline__ void move_tile(uint32_t* sh, uint32_t* g, int rows, int tc, size_t gstride) {
+    const bool vec = ((tc & 3) == 0) && (((uintptr_t)g & 15) == 0) && ((gstride & 3) == 0);
+    if (vec) {
+        const int q4 = tc >> 2, lq = 31 - __clz(q4);
+        const int total = rows * q4;
+        for (int b0 = threadIdx.x; b0 < total; b0 += 8 * blockDim.x) {
+            uint4 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = b0 + u * blockDim.x;
+                if (idx < total) {
+                    const int r = idx >> lq, c = (idx & (q4 - 1)) << 2;
+                    v[u] = TO_SMEM ? *reinterpret_cast<const uint4*>(g + (size_t)r * gstride + c)
+                                   : reinterpret_cast<const uint4*>(sh)[idx];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = b0 + u * blockDim.x;
+                if (idx < total) {
+                    const int r = idx >> lq, c = (idx & (q4 - 1)) << 2;
+                    if (TO_SMEM) reinterpret_cast<uint4*>(sh)[idx] = v[u];
+                    else *reinterpret_cast<uint4*>(g + (size_t)r * gstride + c) = v[u];
+                }
+            }
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < rows * tc; idx += blockDim.x) {
+            uint32_t* gp = g + (size_t)(idx / tc) * gstride + (idx % tc);
+            if (TO_SMEM) sh[idx] = *gp;
+            else *gp = sh[idx];
+        }
+    }
+}
+
+// Stages the twiddles of row stages 0..w2-1 for rows [hi0, hi0 + rpb) as Tw2 pairs:
+// twf[rpb (2^ls - 1) + t] = tw[2^(w1+ls) + hi0 2^ls + t]; with MIRROR, the entries of the
+// mirrored rows in reverse: tw[2^(w1+ls) + (nrows - hi0) 2^ls - 1 - t].
+template <bool MIRROR>
+__device__ __forceinline__ void stage_row_twiddles(Tw2* out, const uint32_t* tw, int rpb, int w1, int w2,
+                                                   uint32_t nrows, uint32_t hi0, uint32_t pinv) {
+    if ((rpb & 3) == 0 && w1 + 0 >= 2) {
+        const int total4 = rpb * ((1 << w2) - 1) / 4;  // groups of 4 entries, stage blocks are multiples of 4
+        for (int g0 = threadIdx.x; g0 < total4; g0 += 4 * blockDim.x) {
+            uint4 v[4];
+            int dst[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int g = g0 + u * blockDim.x;
+                dst[u] = -1;
+                if (g < total4) {
+                    const int ls = 31 - __clz(4 * g / rpb + 1);
+                    const int o = rpb * ((1 << ls) - 1), t = 4 * g - o;
+                    const uint32_t s0 = 1u << (w1 + ls);
+                    const uint32_t src = MIRROR ? s0 + ((nrows - hi0) << ls) - 4 - t : s0 + (hi0 << ls) + t;
+                    v[u] = *reinterpret_cast<const uint4*>(tw + src);
+                    dst[u] = o + t;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (dst[u] < 0) continue;
+                uint32_t w[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+                if (MIRROR) {
+                    const uint32_t t0 = w[0], t1 = w[1];
+                    w[0] = w[3];
+                    w[1] = w[2];
+                    w[2] = t1;
+                    w[3] = t0;
+                }
+                uint4* o4 = reinterpret_cast<uint4*>(out + dst[u]);
+                o4[0] = make_uint4(w[0], w[0] * pinv, w[1], w[1] * pinv);
+                o4[1] = make_uint4(w[2], w[2] * pinv, w[3], w[3] * pinv);
+            }
+        }
+    } else {
+        for (int ls = 0; ls < w2; ++ls) {
+            const int o = rpb * ((1 << ls) - 1), cnt = rpb << ls;
+            const uint32_t s0 = 1u << (w1 + ls);
+            for (int t = threadIdx.x; t < cnt; t += blockDim.x)
+                out[o + t] = make_tw(tw[MIRROR ? s0 + ((nrows - hi0) << ls) - 1 - t : s0 + (hi0 << ls) + t], pinv);
+        }
+    }
 }
 
 }  // namespace
 
-// Column pass: the first w1 stages on a tile of 2^ltc columns x nrows rows of prime
+// Column pass: the first w1 = NB stages on a tile of 2^ltc columns x 2^NB rows of prime
 // blockIdx.y, batch blockIdx.z.  Column stage s, group i uses tw[2^s + i] (forward) or
-// tw[2^(s+1) - 1 - i] (inverse); all of them index below nrows.
-template <bool INV>
+// tw[2^(s+1) - 1 - i] (inverse); all of them index below nrows.  Consecutive threads take
+// consecutive columns, so a warp's 32 lanes hit 32 banks and share one twiddle.
+template <int NB, bool INV>
 __global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restrict__ R, uint32_t col0, int ltc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int nr = (int)P.nrows, w1 = P.w1, tc = 1 << ltc;
-    Tw2* tws = reinterpret_cast<Tw2*>(smem_raw);            // [nrows]
-    uint32_t* sh = reinterpret_cast<uint32_t*>(tws + nr);   // [nrows][tc]
+    constexpr int NR = 1 << NB;
+    const int tc = 1 << ltc;
+    Tw2* tws = reinterpret_cast<Tw2*>(smem_raw);            // [NR]
+    uint32_t* sh = reinterpret_cast<uint32_t*>(tws + NR);   // [NR][tc]
     const int j = (int)blockIdx.y;
     const uint32_t p = P.p[j], pinv = P.pinv[j];
     uint32_t* base = R + ((size_t)blockIdx.z * P.K + j) * P.N + col0 + ((uint32_t)blockIdx.x << ltc);
     const uint32_t* tw = P.tw + (size_t)j * P.N;
 
-    for (int k = threadIdx.x; k < nr; k += blockDim.x) tws[k] = make_tw(tw[k], pinv);
-    for (int idx = threadIdx.x; idx < (nr << ltc); idx += blockDim.x)
-        sh[idx] = base[(size_t)(idx >> ltc) * P.ncols + (idx & (tc - 1))];
+    move_tile<true>(sh, base, NR, tc, P.ncols);
+    for (int k = threadIdx.x; k < NR; k += blockDim.x) tws[k] = make_tw(__ldg(tw + k), pinv);
     __syncthreads();
 
     auto twf = [&](int ls, int gi) { return INV ? tws[(2 << ls) - 1 - gi] : tws[(1 << ls) + gi]; };
-    const int npass = (w1 + 2) / 3;
-    for (int pi = 0; pi < npass; ++pi) {
-        const int ls0 = 3 * (INV ? npass - 1 - pi : pi), r = min(3, w1 - ls0);
-        for (int t = threadIdx.x; t < ((nr >> r) << ltc); t += blockDim.x)
-            radix_group_r<INV>(r, sh + (t & (tc - 1)), tc, w1, ls0, t >> ltc, twf, p);
-        __syncthreads();
-    }
-    for (int idx = threadIdx.x; idx < (nr << ltc); idx += blockDim.x)
-        base[(size_t)(idx >> ltc) * P.ncols + (idx & (tc - 1))] = sh[idx];
+    for_each_pass<NB, 0, INV>([&](auto l0, auto rd) {
+        constexpr int LS0 = decltype(l0)::value, RAD = decltype(rd)::value;
+        for (int t = threadIdx.x; t < ((NR >> RAD) << ltc); t += blockDim.x)
+            radix_group<NB, LS0, RAD, INV>(sh + (t & (tc - 1)), tc, t >> ltc, twf, p);
+    });
+    move_tile<false>(sh, base, NR, tc, P.ncols);
 }
 
 // Row pass over `rpb` consecutive rows of prime blockIdx.y, batch blockIdx.z.
@@ -110,11 +208,12 @@ __global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restric
 // [hi0, hi0 + rpb) those entries are one contiguous run per stage, staged in shared memory
 // as twf[rpb (2^ls - 1) + rr 2^ls + gi].  The inverse twiddle of (hi, gi) is the forward
 // entry of the mirrored row nrows-1-hi at 2^ls-1-gi, staged as twi with the same indexing.
-template <bool FUSED>
+template <int NB, bool FUSED>
 __global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
                                                   int rpb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int w1 = P.w1, w2 = P.w2, nc = (int)P.ncols;
+    constexpr int w2 = NB, nc = 1 << NB;
+    const int w1 = P.w1;
     const int ntw = rpb * (nc - 1);
     Tw2* twf_s = reinterpret_cast<Tw2*>(smem_raw);
     Tw2* twi_s = twf_s + (ntw > 0 ? ntw : 1);
@@ -126,83 +225,127 @@ __global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restric
     uint32_t* rows = R + off;
     const uint32_t* tw = P.tw + (size_t)j * P.N;
 
-    for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) sh[idx] = rows[idx];
-    for (int ls = 0; ls < w2; ++ls) {
-        const int o = rpb * ((1 << ls) - 1), cnt = rpb << ls;
-        const uint32_t s0 = 1u << (w1 + ls);
-        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-            twf_s[o + t] = make_tw(tw[s0 + (hi0 << ls) + t], pinv);
-            if (FUSED) twi_s[o + t] = make_tw(tw[s0 + ((P.nrows - hi0) << ls) - 1 - t], pinv);
-        }
-    }
+    move_tile<true>(sh, rows, 1, rpb * nc, 0);
+    stage_row_twiddles<false>(twf_s, tw, rpb, w1, w2, P.nrows, hi0, pinv);
+    if (FUSED) stage_row_twiddles<true>(twi_s, tw, rpb, w1, w2, P.nrows, hi0, pinv);
     __syncthreads();
 
-    const int npass = (w2 + 2) / 3;
-    for (int pi = 0; pi < npass; ++pi) {
-        const int ls0 = 3 * pi, r = min(3, w2 - ls0), lg = w2 - r;
-        for (int t = threadIdx.x; t < (rpb << lg); t += blockDim.x) {
-            const int rr = t >> lg;
+    for_each_pass<NB, 0, false>([&](auto l0, auto rd) {
+        constexpr int LS0 = decltype(l0)::value, RAD = decltype(rd)::value, LG = NB - RAD;
+        for (int t = threadIdx.x; t < (rpb << LG); t += blockDim.x) {
+            const int rr = t >> LG;
             auto twf = [&](int ls, int gi) { return twf_s[rpb * ((1 << ls) - 1) + (rr << ls) + gi]; };
-            radix_group_r<false>(r, sh + rr * nc, 1, w2, ls0, t & ((1 << lg) - 1), twf, p);
+            radix_group<NB, LS0, RAD, false>(sh + (rr << NB), 1, t & ((1 << LG) - 1), twf, p);
         }
-        __syncthreads();
-    }
+    });
     if (FUSED) {
         const uint32_t* arows = RA + off;
-        for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) {
+        for (int idx = threadIdx.x; idx < (rpb << NB); idx += blockDim.x) {
             const uint32_t a = red_once(red_once(arows[idx], 2 * p), p);   // [0, 4p) -> [0, p)
             sh[idx] = mont_mul(a, sh[idx], p, pinv);                        // (0, 2p)
         }
         __syncthreads();
-        for (int pi = npass - 1; pi >= 0; --pi) {
-            const int ls0 = 3 * pi, r = min(3, w2 - ls0), lg = w2 - r;
-            for (int t = threadIdx.x; t < (rpb << lg); t += blockDim.x) {
-                const int rr = t >> lg;
+        for_each_pass<NB, 0, true>([&](auto l0, auto rd) {
+            constexpr int LS0 = decltype(l0)::value, RAD = decltype(rd)::value, LG = NB - RAD;
+            for (int t = threadIdx.x; t < (rpb << LG); t += blockDim.x) {
+                const int rr = t >> LG;
                 auto twf = [&](int ls, int gi) { return twi_s[rpb * ((1 << ls) - 1) + (rr << ls) + gi]; };
-                radix_group_r<true>(r, sh + rr * nc, 1, w2, ls0, t & ((1 << lg) - 1), twf, p);
+                radix_group<NB, LS0, RAD, true>(sh + (rr << NB), 1, t & ((1 << LG) - 1), twf, p);
             }
-            __syncthreads();
+        });
+    }
+    move_tile<false>(sh, rows, 1, rpb * nc, 0);
+}
+
+namespace {
+
+template <int NB>
+void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
+                    int ltc) {
+    if (inv) k_ntt_cols<NB, true><<<grid, 256, smem, s>>>(P, R, col0, ltc);
+    else k_ntt_cols<NB, false><<<grid, 256, smem, s>>>(P, R, col0, ltc);
+}
+
+template <int NB>
+void launch_rows_nb(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
+                    const uint32_t* RA, int rpb) {
+    if (fused) k_ntt_rows<NB, true><<<grid, 128, smem, s>>>(P, R, RA, rpb);
+    else k_ntt_rows<NB, false><<<grid, 128, smem, s>>>(P, R, RA, rpb);
+}
+
+// Applies f<NB>() for the line length nb in [0, PM_MAX_LINE_LOG].
+template <template <int> class F, class... A>
+void dispatch_nb(int nb, A&&... a) {
+    switch (nb) {
+        case 0: F<0>::run(a...); break;
+        case 1: F<1>::run(a...); break;
+        case 2: F<2>::run(a...); break;
+        case 3: F<3>::run(a...); break;
+        case 4: F<4>::run(a...); break;
+        case 5: F<5>::run(a...); break;
+        case 6: F<6>::run(a...); break;
+        case 7: F<7>::run(a...); break;
+        case 8: F<8>::run(a...); break;
+        case 9: F<9>::run(a...); break;
+        case 10: F<10>::run(a...); break;
+        default: throw_cuda(cudaErrorInvalidValue, "NTT line length above 2^10");
+    }
+}
+
+template <int NB>
+struct ColsF {
+    template <class... A>
+    static void run(A&&... a) { launch_cols_nb<NB>(a...); }
+};
+template <int NB>
+struct RowsF {
+    template <class... A>
+    static void run(A&&... a) { launch_rows_nb<NB>(a...); }
+};
+template <int NB>
+struct AttrF {
+    static void run(int bytes) {
+        const void* fns[4] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>,
+                              (const void*)k_ntt_rows<NB, false>, (const void*)k_ntt_rows<NB, true>};
+        for (const void* f : fns) {
+            const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e != cudaSuccess) throw_cuda(e, "NTT kernel attribute");
         }
     }
-    for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) rows[idx] = sh[idx];
-}
+};
+template <int NB>
+struct ProbeF {
+    static void run() {
+        const void* fns[4] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>,
+                              (const void*)k_ntt_rows<NB, false>, (const void*)k_ntt_rows<NB, true>};
+        for (const void* f : fns) {
+            cudaFuncAttributes fa{};
+            const cudaError_t e = cudaFuncGetAttributes(&fa, f);
+            if (e != cudaSuccess) throw_cuda(e, "NTT kernel image");
+        }
+    }
+};
+
+}  // namespace
 
 void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
                      int ltc) {
-    if (inv) k_ntt_cols<true><<<grid, 256, smem, s>>>(P, R, col0, ltc);
-    else k_ntt_cols<false><<<grid, 256, smem, s>>>(P, R, col0, ltc);
+    dispatch_nb<ColsF>(P.w1, inv, grid, smem, s, P, R, col0, ltc);
 }
 
 void launch_ntt_rows(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
                      const uint32_t* RA, int rpb) {
-    if (fused) k_ntt_rows<true><<<grid, 128, smem, s>>>(P, R, RA, rpb);
-    else k_ntt_rows<false><<<grid, 128, smem, s>>>(P, R, RA, rpb);
+    dispatch_nb<RowsF>(P.w2, fused, grid, smem, s, P, R, RA, rpb);
 }
 
-namespace {
-struct NttKernel {
-    const void* fn;
-    const char* name;
-};
-const NttKernel kNttKernels[] = {{(const void*)k_ntt_cols<false>, "k_ntt_cols<forward>"},
-                                 {(const void*)k_ntt_cols<true>, "k_ntt_cols<inverse>"},
-                                 {(const void*)k_ntt_rows<false>, "k_ntt_rows<forward>"},
-                                 {(const void*)k_ntt_rows<true>, "k_ntt_rows<fused>"}};
-}  // namespace
-
-void ntt_set_smem_limit(int bytes) {
-    for (const NttKernel& k : kNttKernels) {
-        const cudaError_t e = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) throw_cuda(e, k.name);
-    }
+void ntt_set_smem_limit(int bytes, int w1, int w2) {
+    dispatch_nb<AttrF>(w1, bytes);
+    if (w2 != w1) dispatch_nb<AttrF>(w2, bytes);
 }
 
-void ntt_probe_images() {
-    for (const NttKernel& k : kNttKernels) {
-        cudaFuncAttributes fa{};
-        const cudaError_t e = cudaFuncGetAttributes(&fa, k.fn);
-        if (e != cudaSuccess) throw_cuda(e, k.name);
-    }
+void ntt_probe_images(int w1, int w2) {
+    dispatch_nb<ProbeF>(w1);
+    if (w2 != w1) dispatch_nb<ProbeF>(w2);
 }
 
 size_t ntt_cols_smem(const DevPlan& P, int ltc) {

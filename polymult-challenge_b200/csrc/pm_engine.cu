@@ -200,7 +200,7 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
         upload_tables();
         setup_launch_shapes();
         const bool tc_fits = rns_tc_smem(dp_) <= smem_optin_ && crt_tc_smem(dp_) <= smem_optin_ &&
-                             dp_.dec_nrows <= 512 && dp_.crt_nrows <= 512;
+                             plan_.KP <= 128 && dp_.crt_nrows <= 512;
         if (gemm_request == GEMM_TENSOR && !tc_fits)
             throw Unsupported("tensor-core GEMM form does not cover this point (shared memory / TMEM)");
         form_ = (gemm_request == GEMM_PLAIN || !tc_fits) ? GEMM_PLAIN : GEMM_TENSOR;
@@ -292,7 +292,7 @@ void Engine::setup_launch_shapes() {
     // Every kernel may use up to the device's opt-in maximum: contexts for different points
     // share these kernels, so a per-point limit set by one context could fail another's launch.
     const int mx = (int)smem_optin_;
-    ntt_probe_images();
+    ntt_probe_images(plan_.w1, plan_.w2);
     struct Probe {
         const void* fn;
         const char* name;
@@ -305,7 +305,7 @@ void Engine::setup_launch_shapes() {
         cudaFuncAttributes fa{};
         cuda_check(cudaFuncGetAttributes(&fa, pr.fn), (std::string("kernel image ") + pr.name).c_str());
     }
-    ntt_set_smem_limit(mx);
+    ntt_set_smem_limit(mx, plan_.w1, plan_.w2);
     cuda_check(cudaFuncSetAttribute(k_rns_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_crt_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_rns_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
@@ -369,7 +369,8 @@ void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R,
     if (form_ == GEMM_TENSOR) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
-        k_rns_tc<<<grid, 128, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, nb, R);
+        const int bulk = ((uintptr_t)src % 16 == 0) && ((size_t)npos * plan_.L * 4) % 16 == 0;
+        k_rns_tc<<<grid, RNS_TC_THREADS, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, nb, R, bulk);
         cuda_check(cudaGetLastError(), "launch k_rns_tc");
     } else {
         dim3 grid((npos + DEC_TM - 1) / DEC_TM, 1, nb);
@@ -398,7 +399,8 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
     if (form_ == GEMM_TENSOR) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
-        k_crt_tc<<<grid, 128, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out);
+        const int bulk = ch.cw >= 4 && ch.col0 % 4 == 0 && plan_.N % 4 == 0 && ((uintptr_t)R % 16 == 0);
+        k_crt_tc<<<grid, CRT_TC_THREADS, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out, bulk);
         cuda_check(cudaGetLastError(), "launch k_crt_tc");
     } else {
         dim3 grid((npos + CRT_TM - 1) / CRT_TM, 1, nb);

@@ -20,8 +20,9 @@ void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const Dev
                      int ltc);
 void launch_ntt_rows(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
                      const uint32_t* RA, int rpb);
-void ntt_set_smem_limit(int bytes);  // cudaFuncAttributeMaxDynamicSharedMemorySize of all four
-void ntt_probe_images();             // throws CudaError naming a kernel whose image cannot load
+// line lengths 2^w1 (columns) and 2^w2 (rows) select the compile-time specialisations
+void ntt_set_smem_limit(int bytes, int w1, int w2);  // max dynamic shared memory of their kernels
+void ntt_probe_images(int w1, int w2);              // throws CudaError if an image cannot load
 size_t ntt_cols_smem(const DevPlan& P, int ltc);
 size_t ntt_rows_smem(const DevPlan& P, int rpb, bool fused);
 
@@ -35,8 +36,12 @@ size_t crt_plain_smem(const DevPlan& P);
 
 // ---- tensor-core (tcgen05 kind::i8) RNS decomposition and CRT (k_tc.cu)
 constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
-__global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R);
-__global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out);
+__global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R,
+                         int use_bulk);
+__global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
+                         int use_bulk);
+constexpr int RNS_TC_THREADS = 256;  // 8 epilogue warps: 4 TMEM lane quarters x 2 prime halves
+constexpr int CRT_TC_THREADS = 256;  // two threads per coefficient / TMEM lane
 size_t rns_tc_smem(const DevPlan& P);
 size_t crt_tc_smem(const DevPlan& P);
 // TMEM columns to allocate: a power of two >= max(32, n)
@@ -46,8 +51,21 @@ __host__ __device__ inline uint32_t tmem_cols_for(int n) {
     return c;
 }
 
+// Decomposition MMA split: primes [0, KH) -> TMEM columns [0, 4KH), the rest from column
+// dec_half1_col; each half is one commit, so the epilogue of half 0 overlaps half 1's MMA.
+__host__ __device__ inline int dec_half_primes(int KP) {
+    const int h = (KP + 1) / 2;
+    return (h + 3) / 4 * 4;
+}
+__host__ __device__ inline uint32_t dec_half1_col(int n0) { return (uint32_t)((n0 + 31) / 32 * 32); }
+
 // words of one CRT staging row: z needs L + 3 limbs (value < 2^(W + 64)); odd stride
 __host__ __device__ inline int crt_zl(int L) { return L + 3; }
 __host__ __device__ inline int crt_zstride(int L) { return crt_zl(L) | 1; }
+// bytes of the CRT A tile region (also holds the z staging rows after the MMA)
+__host__ __device__ inline size_t crt_a_bytes(const DevPlan& P) {
+    const size_t a = (size_t)TC_M * P.crt_kbytes, z = (size_t)TC_M * crt_zstride(P.L) * 4;
+    return a > z ? a : z;
+}
 
 }  // namespace pm
