@@ -91,6 +91,19 @@ enum pm_stage {
 int pm_time_stages(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, uint32_t count,
                    int reps, void* stream, float* ms_out);
 
+/* No counterpart in the reference.  One device-resident multiply, c = a*b with d_a, d_b, d_c
+ * of N*L words in device memory, that allocates nothing: its residue scratch is a fixed 64 MiB
+ * device array inside this library (held on every GPU that loads the library until exit), so
+ * it serves callers that cannot call cudaMalloc while computing -- e.g. a host framework whose
+ * caching allocator owns the device memory, or a latency-critical path that cannot take
+ * cudaMalloc's implicit synchronisation (pm_run_device may allocate to grow its scratch).
+ * Limit: K*N <= 8,388,608 residue words per operand (N = 65536 up to W = 1747); larger points
+ * return PM_ERR_INVALID.  Asynchronous on `stream`; pm_sync() reports device-side checks.
+ * All calls share the scratch array: calls that overlap on the GPU race, so serialise them.
+ * The first call on a device looks up the array's device address; make it before any stream
+ * capture.  The context must come from an earlier pm_init (which does allocate). */
+int pm_run_device_static(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream);
+
 /* Waits for the context's device work and returns PM_ERR_DEVICE if a device-side check
  * failed since the last call. */
 int pm_sync(pm_context* ctx);

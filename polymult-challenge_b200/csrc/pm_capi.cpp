@@ -6,13 +6,9 @@
 #include <vector>
 
 #include "../../include/polymult_b200.h"
-#include "pm_engine.h"
+#include "pm_context.h"
 
-struct pm_context {
-    pm::Engine* engine;
-};
-
-namespace {
+namespace pm {
 
 thread_local std::string g_last_error;
 
@@ -20,6 +16,13 @@ int fail(int code, const char* what) {
     g_last_error = what ? what : "";
     return code;
 }
+
+}  // namespace pm
+
+using pm::fail;
+using pm::g_last_error;
+
+namespace {
 
 template <class F>
 int guarded(F&& f) {

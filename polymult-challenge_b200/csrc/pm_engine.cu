@@ -482,6 +482,21 @@ void Engine::time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint
     throw_if_status();
 }
 
+void Engine::run_device_with_scratch(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* ra, uint32_t* rb,
+                                     cudaStream_t s) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    const Chunk all{0, plan_.ncols};
+    launch_dec(a, all, 1, ra, s);
+    launch_cols(false, ra, all, 1, s);
+    launch_rows(false, ra, nullptr, 1, s);
+    launch_dec(b, all, 1, rb, s);
+    launch_cols(false, rb, all, 1, s);
+    launch_rows(true, rb, ra, 1, s);
+    launch_cols(true, rb, all, 1, s);
+    launch_crt(rb, all, 1, c, s);
+    cuda_check(cudaGetLastError(), "kernel launch");
+}
+
 uint32_t Engine::take_status() {
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
     uint32_t st = 0;

@@ -71,6 +71,10 @@ class Engine {
     // c[i] = a[i] * b[i] for i < count; operands contiguous [count][N][L] in device memory.
     // Asynchronous on `stream`; check_status() reports device-side check failures.
     void run_device(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t count, cudaStream_t stream);
+    // One multiply with residue scratch supplied by the caller (two arrays of K*N words);
+    // allocates nothing.  Asynchronous on `stream`.
+    void run_device_with_scratch(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* ra, uint32_t* rb,
+                                 cudaStream_t stream);
     // Per-kernel mean durations (ms) of `reps` groups of `count` multiplies (CUDA events).
     void time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t count, int reps, cudaStream_t s,
                      float* ms_out);

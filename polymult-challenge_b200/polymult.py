@@ -77,6 +77,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_time_stages.argtypes = [vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_int, vp,
                                    ctypes.POINTER(ctypes.c_float)]
     lib.pm_time_stages.restype = ctypes.c_int
+    lib.pm_run_device_static.argtypes = [vp, vp, vp, vp, vp]
+    lib.pm_run_device_static.restype = ctypes.c_int
     lib.pm_sync.argtypes = [vp]
     lib.pm_sync.restype = ctypes.c_int
     lib.pm_free.argtypes = [vp]
@@ -146,6 +148,10 @@ class Multiplier:
     def multiply_device(self, a_ptr: int, b_ptr: int, c_ptr: int, count: int = 1, stream: int = 0):
         """Device-resident operands [count][N][L]; asynchronous on `stream` (cudaStream_t as int)."""
         _check(load().pm_run_device(self._h, a_ptr, b_ptr, c_ptr, count, stream or None))
+
+    def multiply_device_static(self, a_ptr: int, b_ptr: int, c_ptr: int, stream: int = 0):
+        """One device-resident multiply that allocates nothing (pm_run_device_static)."""
+        _check(load().pm_run_device_static(self._h, a_ptr, b_ptr, c_ptr, stream or None))
 
     def time_stages(self, a_ptr: int, b_ptr: int, c_ptr: int, count: int = 1, reps: int = 3, stream: int = 0):
         """Mean per-kernel durations (ms) in launch order, keyed by STAGES."""
