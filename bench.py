@@ -234,6 +234,28 @@ def run_reference(args):
 # ------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------
+def pcie_bandwidth(torch, nbytes_h2d, nbytes_d2h, reps=5):
+    """Pinned cudaMemcpyAsync bandwidth (GB/s) at the call's transfer sizes, CUDA events."""
+    out = {}
+    for name, n in (("h2d", nbytes_h2d), ("d2h", nbytes_d2h)):
+        h = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        d = torch.empty(n, dtype=torch.uint8, device="cuda")
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if name == "h2d":
+                d.copy_(h, non_blocking=True)
+            else:
+                h.copy_(d, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        out[name] = n / (best / 1000.0) / 1e9
+    return out
+
+
 def time_device(torch, m, da, db, dc, batch, steps, warm):
     stream = torch.cuda.current_stream()
     for _ in range(warm):
@@ -328,10 +350,14 @@ def run_ours(args):
     e2e_s = max_over_ranks(sum(lat), world)
     e2e_ok = bool(np.array_equal(out, dc[0].cpu().numpy().view(np.uint32)))
     lat_ms = sorted(x * 1000 for x in lat)
+    bw = pcie_bandwidth(torch, 2 * N * L * 4, N * L * 4)
+    floor_ms = (2 * N * L * 4 / (bw["h2d"] * 1e9) + N * L * 4 / (bw["d2h"] * 1e9)) * 1000
     e2e = {"value": world * args.e2e_steps / e2e_s, "unit": "mults/s", "h2d_bytes_per_step": 2 * N * L * 4,
            "d2h_bytes_per_step": N * L * 4, "p50_ms": round(lat_ms[len(lat_ms) // 2], 4),
            "p99_ms": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 4),
-           "steps": args.e2e_steps, "matches_device_path": e2e_ok}
+           "steps": args.e2e_steps, "matches_device_path": e2e_ok,
+           "pcie_gbs": {k: round(v, 2) for k, v in bw.items()}, "pcie_floor_ms": round(floor_ms, 4),
+           "p50_over_floor": round(lat_ms[len(lat_ms) // 2] / floor_ms, 3)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

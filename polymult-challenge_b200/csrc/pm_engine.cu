@@ -15,6 +15,9 @@
 #include "pm_engine.h"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "pm_kernels.cuh"
@@ -35,62 +38,76 @@ void throw_cuda(cudaError_t e, const char* what) { throw CudaError(std::string(w
 // ---------------------------------------------------------------------------------------
 // host pool
 // ---------------------------------------------------------------------------------------
-HostPool::HostPool(int workers) {
+HostPool::HostPool(int workers, int idle_us) : idle_us_(idle_us) {
     for (int i = 0; i < workers; ++i) threads_.emplace_back([this] { loop(); });
 }
 
 HostPool::~HostPool() {
+    stop_.store(true);
     {
         std::lock_guard<std::mutex> lk(m_);
-        stop_ = true;
+        cv_.notify_all();
     }
-    cv_.notify_all();
     for (auto& t : threads_) t.join();
+}
+
+// Claims and runs one task of generation `gen`; false when there is none left to claim.
+bool HostPool::work_once(uint64_t gen) {
+    uint64_t c = claim_.load(std::memory_order_acquire);
+    for (;;) {
+        if ((c >> 32) != gen || (int)(uint32_t)c >= n_.load(std::memory_order_acquire)) return false;
+        if (claim_.compare_exchange_weak(c, c + 1, std::memory_order_acq_rel, std::memory_order_acquire)) break;
+    }
+    (*fn_)((int)(uint32_t)c);
+    done_.fetch_add(1, std::memory_order_acq_rel);
+    return true;
 }
 
 void HostPool::run(int n, const std::function<void(int)>& fn) {
     if (n <= 0) return;
-    {
+    fn_ = &fn;
+    n_.store(n, std::memory_order_relaxed);
+    done_.store(0, std::memory_order_relaxed);
+    const uint64_t gen = (claim_.load(std::memory_order_relaxed) >> 32) + 1;
+    claim_.store(gen << 32, std::memory_order_release);
+    if (sleepers_.load() > 0) {
         std::lock_guard<std::mutex> lk(m_);
-        fn_ = &fn;
-        n_ = n;
-        next_.store(0);
-        finished_ = 0;
-        ++gen_;
+        cv_.notify_all();
     }
-    cv_.notify_all();
-    int done_here = 0;
-    for (int i = next_.fetch_add(1); i < n; i = next_.fetch_add(1)) {
-        fn(i);
-        ++done_here;
+    while (work_once(gen)) {
     }
-    std::unique_lock<std::mutex> lk(m_);
-    finished_ += done_here;
-    done_cv_.wait(lk, [&] { return finished_ >= n_; });
-    fn_ = nullptr;
+    while (done_.load(std::memory_order_acquire) < n) {
+#if defined(__x86_64__)
+        __builtin_ia32_pause();
+#endif
+    }
 }
 
 void HostPool::loop() {
-    uint64_t seen = 0;
-    for (;;) {
-        const std::function<void(int)>* fn;
-        int n;
-        {
-            std::unique_lock<std::mutex> lk(m_);
-            cv_.wait(lk, [&] { return stop_ || (gen_ != seen && fn_ != nullptr); });
-            if (stop_) return;
-            seen = gen_;
-            fn = fn_;
-            n = n_;
+    using clock = std::chrono::steady_clock;
+    auto last = clock::now();
+    uint32_t spins = 0;
+    while (!stop_.load(std::memory_order_relaxed)) {
+        const uint64_t gen = claim_.load(std::memory_order_acquire) >> 32;
+        if (work_once(gen)) {
+            last = clock::now();
+            continue;
         }
-        int done_here = 0;
-        for (int i = next_.fetch_add(1); i < n; i = next_.fetch_add(1)) {
-            (*fn)(i);
-            ++done_here;
+#if defined(__x86_64__)
+        __builtin_ia32_pause();
+#endif
+        if ((++spins & 1023u) == 0 && clock::now() - last > std::chrono::microseconds(idle_us_)) {
+            sleepers_.fetch_add(1);
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait_for(lk, std::chrono::milliseconds(100), [&] {
+                    const uint64_t c = claim_.load();
+                    return stop_.load() || ((c >> 32) != gen && (int)(uint32_t)c < n_.load());
+                });
+            }
+            sleepers_.fetch_sub(1);
+            last = clock::now();
         }
-        std::lock_guard<std::mutex> lk(m_);
-        finished_ += done_here;
-        if (finished_ >= n_) done_cv_.notify_all();
     }
 }
 
@@ -240,6 +257,7 @@ Engine::~Engine() {
     for (auto h : h_in_)
         if (h) cudaFreeHost(h);
     if (h_out_) cudaFreeHost(h_out_);
+    if (h_status_) cudaFreeHost(h_status_);
 }
 
 void Engine::upload_tables() {
@@ -327,7 +345,7 @@ void Engine::ensure_scratch(uint32_t group) {
 void Engine::setup_host_pipeline() {
     const uint32_t nc = plan_.ncols;
     cin_ = make_chunks(nc, {32, 32, 16}, 8, {});
-    cout_ = make_chunks(nc, {64, 64, 32}, 16, {32, 64, 64});
+    cout_ = make_chunks(nc, {64, 32}, 8, {32, 64});
     const size_t bytes = plan_.coeff_words() * 4;
     for (int i = 0; i < 2; ++i) {
         d_in_[i] = dev_alloc<uint32_t>(dev_allocs_, plan_.coeff_words(), nullptr);
@@ -335,6 +353,9 @@ void Engine::setup_host_pipeline() {
     }
     d_out_ = dev_alloc<uint32_t>(dev_allocs_, plan_.coeff_words(), nullptr);
     cuda_check(cudaHostAlloc(&h_out_, bytes, cudaHostAllocDefault), "cudaHostAlloc");
+    cuda_check(cudaHostAlloc(&h_status_, 16, cudaHostAllocDefault), "cudaHostAlloc");
+    *h_status_ = 0;
+    profile_ = std::getenv("POLYMULT_PROFILE") != nullptr;
     for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
@@ -348,7 +369,8 @@ void Engine::setup_host_pipeline() {
     mk(ev_out_, cout_.size());
     cuda_check(cudaEventCreateWithFlags(&ev_row_a_, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
-    pool_.reset(new HostPool(std::max(0, std::min(12, usable_cpus() - 2))));
+    // 8 copying threads saturate this class of host's memory bandwidth; more only contend
+    pool_.reset(new HostPool(std::max(0, std::min(7, usable_cpus() - 2))));
 }
 
 int Engine::kernel_launches_per_group() const { return plan_.w1 > 0 ? 8 : 6; }
@@ -542,7 +564,12 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         });
     };
     uint32_t* dR[2] = {d_ra_, d_rb_};
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    auto us = [&](clk::time_point t) { return std::chrono::duration<double, std::micro>(t - t0).count(); };
+    clk::time_point t_stage0, t_inputs, t_first_out, t_last_out;
     stage(0);
+    t_stage0 = clk::now();
     for (int i = 0; i < nin; ++i) {
         const int P = i / na, ci = i % na;
         const Chunk ch = cin_[ci];
@@ -578,9 +605,16 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         cuda_check(cudaMemcpyAsync(h_out_ + off, d_out_ + off, words * 4, cudaMemcpyDeviceToHost, s_d2h_), "D2H");
         cuda_check(cudaEventRecord(ev_out_[oc], s_d2h_), "record");
     }
+    // device status word -> pinned memory behind the last D2H (s_d2h has waited on every CRT)
+    cuda_check(cudaMemcpyAsync(h_status_, dp_.status, 4, cudaMemcpyDeviceToHost, s_d2h_), "status D2H");
+    cuda_check(cudaMemsetAsync(dp_.status, 0, 4, s_d2h_), "status clear");
+    cuda_check(cudaEventRecord(ev_out_.back(), s_d2h_), "record");
     cuda_check(cudaGetLastError(), "kernel launch");
+    t_inputs = clk::now();
     for (size_t oc = 0; oc < cout_.size(); ++oc) {
         cuda_check(cudaEventSynchronize(ev_out_[oc]), "D2H chunk");
+        if (oc == 0) t_first_out = clk::now();
+        if (oc + 1 == cout_.size()) t_last_out = clk::now();
         const Chunk ch = cout_[oc];
         const uint32_t* srcc = h_out_ + (size_t)ch.col0 * nrows * L;
         const size_t seg = (size_t)ch.cw * L;
@@ -590,7 +624,19 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
                 stream_copy(c + ((size_t)r * ncols + ch.col0) * L, srcc + r * seg, seg * 4);
         });
     }
-    throw_if_status();
+    if (profile_)
+        std::fprintf(stderr,
+                     "polymult: stage0 %.1f us | inputs issued %.1f | first out %.1f | last out %.1f | done %.1f\n",
+                     us(t_stage0), us(t_inputs), us(t_first_out), us(t_last_out), us(clk::now()));
+    const uint32_t st = *h_status_;
+    if (st) {
+        *h_status_ = 0;
+        std::string what = "device-side check failed:";
+        if (st & DEV_ERR_CRT_BOUND) what += " CRT estimate outside its exactness bound;";
+        if (st & DEV_ERR_FOLD) what += " delta-fold did not converge;";
+        if (st & DEV_ERR_WAIT) what += " tensor-core wait timed out;";
+        throw DeviceCheckError(what);
+    }
 }
 
 }  // namespace pm

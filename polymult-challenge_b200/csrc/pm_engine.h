@@ -35,24 +35,31 @@ void cuda_check(cudaError_t e, const char* what);
 
 // Host worker pool for the pageable <-> pinned staging copies.  run(n, fn) executes
 // fn(0..n-1) across the workers and the calling thread and returns when all are done.
+// Workers spin between jobs (a job every few tens of microseconds is the pipeline's rhythm;
+// a condition-variable wake-up per job would cost more than the copy) and fall back to
+// sleeping after `idle_us` without work.  Task indices are claimed with a compare-and-swap
+// on (generation << 32 | next index), so a worker still finishing an old job can never take
+// a task of the next one.
 class HostPool {
   public:
-    explicit HostPool(int workers);
+    explicit HostPool(int workers, int idle_us = 200000);
     ~HostPool();
     void run(int n, const std::function<void(int)>& fn);
     int size() const { return (int)threads_.size() + 1; }
 
   private:
     void loop();
+    bool work_once(uint64_t gen);
     std::vector<std::thread> threads_;
-    std::mutex m_;
-    std::condition_variable cv_, done_cv_;
+    std::atomic<uint64_t> claim_{0};     // (generation << 32) | next task index
+    std::atomic<int> done_{0};
+    std::atomic<int> n_{0};
+    std::atomic<bool> stop_{false};
+    std::atomic<int> sleepers_{0};
     const std::function<void(int)>* fn_ = nullptr;
-    int n_ = 0;
-    std::atomic<int> next_{0};
-    int finished_ = 0;
-    uint64_t gen_ = 0;
-    bool stop_ = false;
+    int idle_us_;
+    std::mutex m_;
+    std::condition_variable cv_;
 };
 
 enum GemmForm : int { GEMM_AUTO = 0, GEMM_PLAIN = 1, GEMM_TENSOR = 2 };
@@ -139,6 +146,8 @@ class Engine {
     cudaStream_t s_comp_[3] = {nullptr, nullptr, nullptr};
     cudaStream_t s_h2d_ = nullptr, s_d2h_ = nullptr;
     std::vector<cudaEvent_t> ev_in_, ev_done_in_, ev_crt_, ev_out_;
+    uint32_t* h_status_ = nullptr;  // pinned copy of the device status word, written after each run_host
+    bool profile_ = false;          // POLYMULT_PROFILE: per-call host phase timeline on stderr
     cudaEvent_t ev_row_a_ = nullptr, ev_fused_ = nullptr;
     std::unique_ptr<HostPool> pool_;
 };
