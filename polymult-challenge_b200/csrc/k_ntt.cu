@@ -62,6 +62,109 @@ __device__ __forceinline__ void radix_group(uint32_t* line, int es, int g, const
     for (int e = 0; e < G; ++e) b[e * step] = v[e];
 }
 
+// Row tiles live in shared memory swizzled within each row: element x of a row sits at
+// swz(x) = x ^ (((x >> 5) & 7) << 2).  The XOR only touches bits 2-4, so aligned runs of 4
+// stay contiguous (16-byte vector access), and with the thread mapping of k_ntt_rows every
+// radix pass of a 256-point row is free of bank conflicts: the pass at stage 3 (elements 4
+// apart) spreads its 8 high index values over the bank bits 2-4, and the pass at stage 6
+// (4 contiguous elements per thread) uses 16-byte loads.
+__device__ __forceinline__ int swz(int x) { return x ^ (((x >> 5) & 7) << 2); }
+
+template <int RAD, int LS0, bool INV, class TwF>
+__device__ __forceinline__ void radix_butterflies(uint32_t (&v)[1 << RAD], int hi, const TwF& twf, uint32_t p) {
+    constexpr int G = 1 << RAD;
+    if (!INV) {
+#pragma unroll
+        for (int k = 0; k < RAD; ++k) {
+            const int h = G >> (k + 1);
+#pragma unroll
+            for (int m = 0; m < (1 << k); ++m) {
+                const Tw2 w = twf(LS0 + k, (hi << k) | m);
+#pragma unroll
+                for (int i = 0; i < h; ++i) bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = RAD - 1; k >= 0; --k) {
+            const int h = G >> (k + 1);
+#pragma unroll
+            for (int m = 0; m < (1 << k); ++m) {
+                const Tw2 w = twf(LS0 + k, (hi << k) | m);
+#pragma unroll
+                for (int i = 0; i < h; ++i) bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
+            }
+        }
+    }
+}
+
+// radix_group for one swizzled row (element stride 1).
+template <int NB, int LS0, int RAD, bool INV, class TwF>
+__device__ __forceinline__ void radix_group_row(uint32_t* row, int g, const TwF& twf, uint32_t p) {
+    constexpr int G = 1 << RAD;
+    constexpr int SUB = NB - LS0 - RAD;
+    const int lo = g & ((1 << SUB) - 1), hi = g >> SUB;
+    const int x0 = (hi << (NB - LS0)) | lo;
+    uint32_t v[G];
+    if constexpr (SUB == 0 && RAD >= 2) {
+#pragma unroll
+        for (int q = 0; q < G / 4; ++q) {
+            const uint4 u = *reinterpret_cast<const uint4*>(row + swz(x0 + 4 * q));
+            v[4 * q] = u.x;
+            v[4 * q + 1] = u.y;
+            v[4 * q + 2] = u.z;
+            v[4 * q + 3] = u.w;
+        }
+    } else if constexpr (SUB == 0 && RAD == 1) {
+        const uint2 u = *reinterpret_cast<const uint2*>(row + swz(x0));
+        v[0] = u.x;
+        v[1] = u.y;
+    } else {
+#pragma unroll
+        for (int e = 0; e < G; ++e) v[e] = row[swz(x0 + (e << SUB))];
+    }
+    radix_butterflies<RAD, LS0, INV>(v, hi, twf, p);
+    if constexpr (SUB == 0 && RAD >= 2) {
+#pragma unroll
+        for (int q = 0; q < G / 4; ++q)
+            *reinterpret_cast<uint4*>(row + swz(x0 + 4 * q)) = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    } else if constexpr (SUB == 0 && RAD == 1) {
+        *reinterpret_cast<uint2*>(row + swz(x0)) = make_uint2(v[0], v[1]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < G; ++e) row[swz(x0 + (e << SUB))] = v[e];
+    }
+}
+
+// rows [0, rpb) x 2^NB words between global (contiguous) and shared (swizzled rows),
+// 16-byte vectors, eight in flight per thread.  Requires 2^NB >= 4.
+template <int NB, bool TO_SMEM>
+__device__ __forceinline__ void move_rows(uint32_t* sh, uint32_t* g, int rpb) {
+    constexpr int Q = (1 << NB) / 4;  // vectors per row
+    const int total = rpb * Q;
+    for (int b0 = threadIdx.x; b0 < total; b0 += 8 * blockDim.x) {
+        uint4 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = b0 + u * blockDim.x;
+            if (q < total) {
+                const int rr = q / Q, x = 4 * (q % Q);
+                v[u] = TO_SMEM ? *reinterpret_cast<const uint4*>(g + 4 * (size_t)q)
+                               : *reinterpret_cast<const uint4*>(sh + (rr << NB) + swz(x));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int q = b0 + u * blockDim.x;
+            if (q < total) {
+                const int rr = q / Q, x = 4 * (q % Q);
+                if (TO_SMEM) *reinterpret_cast<uint4*>(sh + (rr << NB) + swz(x)) = v[u];
+                else *reinterpret_cast<uint4*>(g + 4 * (size_t)q) = v[u];
+            }
+        }
+    }
+}
+
 template <int V>
 using IntC = std::integral_constant<int, V>;
 
@@ -214,18 +317,21 @@ __global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restric
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int w2 = NB, nc = 1 << NB;
     const int w1 = P.w1;
-    const int ntw = rpb * (nc - 1);
+    const int ntw = ntt_row_twiddle_slots(rpb, nc);
     Tw2* twf_s = reinterpret_cast<Tw2*>(smem_raw);
-    Tw2* twi_s = twf_s + (ntw > 0 ? ntw : 1);
-    uint32_t* sh = reinterpret_cast<uint32_t*>(twi_s + (FUSED ? (ntw > 0 ? ntw : 1) : 0));
+    Tw2* twi_s = twf_s + ntw;
+    uint32_t* sh = reinterpret_cast<uint32_t*>(twi_s + (FUSED ? ntw : 0));
     const int j = (int)blockIdx.y;
     const uint32_t p = P.p[j], pinv = P.pinv[j];
     const uint32_t hi0 = blockIdx.x * (uint32_t)rpb;
     const size_t off = ((size_t)blockIdx.z * P.K + j) * P.N + (size_t)hi0 * nc;
     uint32_t* rows = R + off;
     const uint32_t* tw = P.tw + (size_t)j * P.N;
+    constexpr bool VEC = nc >= 4;
 
-    move_tile<true>(sh, rows, 1, rpb * nc, 0);
+    if constexpr (VEC) move_rows<NB, true>(sh, rows, rpb);
+    else
+        for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) sh[idx] = rows[idx];
     stage_row_twiddles<false>(twf_s, tw, rpb, w1, w2, P.nrows, hi0, pinv);
     if (FUSED) stage_row_twiddles<true>(twi_s, tw, rpb, w1, w2, P.nrows, hi0, pinv);
     __syncthreads();
@@ -235,14 +341,29 @@ __global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restric
         for (int t = threadIdx.x; t < (rpb << LG); t += blockDim.x) {
             const int rr = t >> LG;
             auto twf = [&](int ls, int gi) { return twf_s[rpb * ((1 << ls) - 1) + (rr << ls) + gi]; };
-            radix_group<NB, LS0, RAD, false>(sh + (rr << NB), 1, t & ((1 << LG) - 1), twf, p);
+            radix_group_row<NB, LS0, RAD, false>(sh + (rr << NB), t & ((1 << LG) - 1), twf, p);
         }
     });
     if (FUSED) {
         const uint32_t* arows = RA + off;
-        for (int idx = threadIdx.x; idx < (rpb << NB); idx += blockDim.x) {
-            const uint32_t a = red_once(red_once(arows[idx], 2 * p), p);   // [0, 4p) -> [0, p)
-            sh[idx] = mont_mul(a, sh[idx], p, pinv);                        // (0, 2p)
+        if constexpr (VEC) {
+            for (int q = threadIdx.x; q < rpb * nc / 4; q += blockDim.x) {
+                const int rr = q / (nc / 4), x = 4 * (q % (nc / 4));
+                const uint4 a4 = *reinterpret_cast<const uint4*>(arows + 4 * (size_t)q);
+                uint4* s4 = reinterpret_cast<uint4*>(sh + (rr << NB) + swz(x));
+                uint4 b4 = *s4;
+                // a in [0, 4p) -> [0, p); Montgomery product (0, 2p)
+                b4.x = mont_mul(red_once(red_once(a4.x, 2 * p), p), b4.x, p, pinv);
+                b4.y = mont_mul(red_once(red_once(a4.y, 2 * p), p), b4.y, p, pinv);
+                b4.z = mont_mul(red_once(red_once(a4.z, 2 * p), p), b4.z, p, pinv);
+                b4.w = mont_mul(red_once(red_once(a4.w, 2 * p), p), b4.w, p, pinv);
+                *s4 = b4;
+            }
+        } else {
+            for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) {
+                const uint32_t a = red_once(red_once(arows[idx], 2 * p), p);
+                sh[idx] = mont_mul(a, sh[idx], p, pinv);
+            }
         }
         __syncthreads();
         for_each_pass<NB, 0, true>([&](auto l0, auto rd) {
@@ -250,11 +371,13 @@ __global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restric
             for (int t = threadIdx.x; t < (rpb << LG); t += blockDim.x) {
                 const int rr = t >> LG;
                 auto twf = [&](int ls, int gi) { return twi_s[rpb * ((1 << ls) - 1) + (rr << ls) + gi]; };
-                radix_group<NB, LS0, RAD, true>(sh + (rr << NB), 1, t & ((1 << LG) - 1), twf, p);
+                radix_group_row<NB, LS0, RAD, true>(sh + (rr << NB), t & ((1 << LG) - 1), twf, p);
             }
         });
     }
-    move_tile<false>(sh, rows, 1, rpb * nc, 0);
+    if constexpr (VEC) move_rows<NB, false>(sh, rows, rpb);
+    else
+        for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) rows[idx] = sh[idx];
 }
 
 namespace {
@@ -353,7 +476,7 @@ size_t ntt_cols_smem(const DevPlan& P, int ltc) {
 }
 
 size_t ntt_rows_smem(const DevPlan& P, int rpb, bool fused) {
-    const size_t ntw = std::max<size_t>(1, (size_t)rpb * (P.ncols - 1));
+    const size_t ntw = (size_t)ntt_row_twiddle_slots(rpb, (int)P.ncols);
     return ntw * sizeof(Tw2) * (fused ? 2 : 1) + (size_t)rpb * P.ncols * 4;
 }
 

@@ -24,6 +24,12 @@ void launch_ntt_rows(bool fused, dim3 grid, size_t smem, cudaStream_t s, const D
 void ntt_set_smem_limit(int bytes, int w1, int w2);  // max dynamic shared memory of their kernels
 void ntt_probe_images(int w1, int w2);              // throws CudaError if an image cannot load
 size_t ntt_cols_smem(const DevPlan& P, int ltc);
+// Tw2 slots per twiddle array of a row-pass CTA: rpb (ncols - 1), at least 1, rounded up to
+// even so that the row tile that follows the arrays starts 16-byte aligned
+__host__ __device__ inline int ntt_row_twiddle_slots(int rpb, int ncols) {
+    const int n = rpb * (ncols - 1);
+    return ((n > 0 ? n : 1) + 1) & ~1;
+}
 size_t ntt_rows_smem(const DevPlan& P, int rpb, bool fused);
 
 // ---- plain (CUDA-core) RNS decomposition and CRT (k_rns.cu)
