@@ -6,12 +6,20 @@
 // psi^-bitrev(2^s+i) = -psi^bitrev(2^s+2^s-1-i); solve.cu:204-378), organised differently:
 //   * every stage uses Harvey lazy butterflies and Montgomery-Shoup twiddle products
 //     (pm_device.cuh), so no butterfly reduces to [0, p);
-//   * twiddles come from one table tw[j][k] = psi_j^bitrev(k) R (mod p_j); a row-pass CTA
-//     stages the forward and mirrored twiddles of its rows in shared memory with their
-//     Shoup companions, instead of forming trow * tsmall with a Montgomery product at every
-//     butterfly (solve.cu:286-338);
-//   * column tiles are 32 columns wide (128-byte row segments) so that a warp reads whole
-//     lines and its 32 lanes hit 32 different banks.
+//   * twiddles come from one table tw[j][k] = psi_j^bitrev(k) R (mod p_j), read directly
+//     (row pass) or staged once per CTA with their Shoup companions (column pass), instead of
+//     forming trow * tsmall with a Montgomery product at every butterfly (solve.cu:286-338);
+//   * a line of 2^NB elements is transformed in PHASES of up to RB = 4 stages.  In a phase a
+//     thread holds 16 elements of the line in registers -- the 16 values of the 4 index bits
+//     [b0, b0 + 4) that the phase's stages pair up -- and runs a radix-16 butterfly network on
+//     them with compile-time indexing.  Between phases the elements are exchanged through
+//     shared memory once (a 256-point row: load -> 4 stages -> exchange -> 4 stages -> store),
+//     where the previous design went through shared memory at every radix-8 pass.
+//
+// Phase k of an NB-bit line covers stage bits NB-1-4k down to b0_k = max(0, NB - 4(k+1));
+// its registers hold index bits [b0_k, b0_k + 4) and the thread's position supplies the
+// rest (low bits below b0_k, high bits above).  The last phase of a line whose length is
+// not a power of 16 re-uses bits [0, 4) and skips the stages an earlier phase has done.
 #include <type_traits>
 
 #include "pm_kernels.cuh"
@@ -19,365 +27,322 @@
 namespace pm {
 namespace {
 
-// Radix-2^RAD group g of the pass that starts at local stage LS0 of a line of 2^NB elements
-// at element stride es (all shapes compile-time except the stride).  The group's elements are
-// idx_e = (hi << (NB - LS0)) | (e << SUB) | lo with SUB = NB - LS0 - RAD, lo = g mod 2^SUB,
-// hi = g >> SUB.  Local stage LS0 + k pairs e and e + 2^(RAD-1-k); the twiddle argument (the
-// stage's group index within the line) is (hi << k) | (e >> (RAD - k)).  twf(ls, gi) returns
-// the twiddle (for INV, already the mirrored one).
-template <int NB, int LS0, int RAD, bool INV, class TwF>
-__device__ __forceinline__ void radix_group(uint32_t* line, int es, int g, const TwF& twf, uint32_t p) {
-    constexpr int G = 1 << RAD;
-    constexpr int SUB = NB - LS0 - RAD;
-    const int lo = g & ((1 << SUB) - 1), hi = g >> SUB;
-    uint32_t* b = line + ((hi << (NB - LS0)) | lo) * es;
-    const int step = es << SUB;
-    uint32_t v[G];
-#pragma unroll
-    for (int e = 0; e < G; ++e) v[e] = b[e * step];
-    if (!INV) {
-#pragma unroll
-        for (int k = 0; k < RAD; ++k) {
-            const int h = G >> (k + 1);
-#pragma unroll
-            for (int m = 0; m < (1 << k); ++m) {
-                const Tw2 w = twf(LS0 + k, (hi << k) | m);
-#pragma unroll
-                for (int i = 0; i < h; ++i) bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
-            }
-        }
-    } else {
-#pragma unroll
-        for (int k = RAD - 1; k >= 0; --k) {
-            const int h = G >> (k + 1);
-#pragma unroll
-            for (int m = 0; m < (1 << k); ++m) {
-                const Tw2 w = twf(LS0 + k, (hi << k) | m);
-#pragma unroll
-                for (int i = 0; i < h; ++i) bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
-            }
-        }
-    }
-#pragma unroll
-    for (int e = 0; e < G; ++e) b[e * step] = v[e];
-}
+template <int NB>
+struct LineCfg {
+    static constexpr int RB = NB < 4 ? NB : 4;      // index bits held in registers
+    static constexpr int E = 1 << RB;               // elements per thread
+    static constexpr int NPH = RB == 0 ? 0 : (NB + RB - 1) / RB;  // phases (none for a 1-point line)
+    __host__ __device__ static constexpr int b0(int k) { return NB - RB * (k + 1) > 0 ? NB - RB * (k + 1) : 0; }
+    // first local stage of phase k (local stage t pairs register bit RB-1-t)
+    __host__ __device__ static constexpr int t0(int k) { return b0(k) + RB - 1 - (NB - 1 - RB * k); }
+    // global stage index of local stage t of phase k: ls = NB - 1 - (b0 + RB - 1 - t)
+    __host__ __device__ static constexpr int ls(int k, int t) { return NB - b0(k) - RB + t; }
+};
 
-// Row tiles live in shared memory swizzled within each row: element x of a row sits at
-// swz(x) = x ^ (((x >> 5) & 7) << 2).  The XOR only touches bits 2-4, so aligned runs of 4
-// stay contiguous (16-byte vector access), and with the thread mapping of k_ntt_rows every
-// radix pass of a 256-point row is free of bank conflicts: the pass at stage 3 (elements 4
-// apart) spreads its 8 high index values over the bank bits 2-4, and the pass at stage 6
-// (4 contiguous elements per thread) uses 16-byte loads.
-__device__ __forceinline__ int swz(int x) { return x ^ (((x >> 5) & 7) << 2); }
-
-template <int RAD, int LS0, bool INV, class TwF>
-__device__ __forceinline__ void radix_butterflies(uint32_t (&v)[1 << RAD], int hi, const TwF& twf, uint32_t p) {
-    constexpr int G = 1 << RAD;
-    if (!INV) {
+// Forward (CT) radix network on v[] over local stages t0..RB-1 of one phase; tw(t, gi)
+// returns the twiddle of local stage t, group gi = (hi << t) | m (hi is folded in by tw).
+template <int RB, int T0, class TwF>
+__device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const TwF& tw, uint32_t p) {
 #pragma unroll
-        for (int k = 0; k < RAD; ++k) {
-            const int h = G >> (k + 1);
+    for (int t = T0; t < RB; ++t) {
+        const int h = (1 << RB) >> (t + 1);
 #pragma unroll
-            for (int m = 0; m < (1 << k); ++m) {
-                const Tw2 w = twf(LS0 + k, (hi << k) | m);
+        for (int m = 0; m < (1 << t); ++m) {
+            const Tw2 w = tw(t, m);
 #pragma unroll
-                for (int i = 0; i < h; ++i) bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
-            }
-        }
-    } else {
-#pragma unroll
-        for (int k = RAD - 1; k >= 0; --k) {
-            const int h = G >> (k + 1);
-#pragma unroll
-            for (int m = 0; m < (1 << k); ++m) {
-                const Tw2 w = twf(LS0 + k, (hi << k) | m);
-#pragma unroll
-                for (int i = 0; i < h; ++i) bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
-            }
+            for (int i = 0; i < h; ++i) bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
         }
     }
 }
 
-// radix_group for one swizzled row (element stride 1).
-template <int NB, int LS0, int RAD, bool INV, class TwF>
-__device__ __forceinline__ void radix_group_row(uint32_t* row, int g, const TwF& twf, uint32_t p) {
-    constexpr int G = 1 << RAD;
-    constexpr int SUB = NB - LS0 - RAD;
-    const int lo = g & ((1 << SUB) - 1), hi = g >> SUB;
-    const int x0 = (hi << (NB - LS0)) | lo;
-    uint32_t v[G];
-    if constexpr (SUB == 0 && RAD >= 2) {
+// Inverse (GS) network, local stages RB-1 down to T0, mirrored twiddles from tw(t, m).
+template <int RB, int T0, class TwF>
+__device__ __forceinline__ void radix_inv(uint32_t (&v)[1 << RB], const TwF& tw, uint32_t p) {
 #pragma unroll
-        for (int q = 0; q < G / 4; ++q) {
-            const uint4 u = *reinterpret_cast<const uint4*>(row + swz(x0 + 4 * q));
-            v[4 * q] = u.x;
-            v[4 * q + 1] = u.y;
-            v[4 * q + 2] = u.z;
-            v[4 * q + 3] = u.w;
-        }
-    } else if constexpr (SUB == 0 && RAD == 1) {
-        const uint2 u = *reinterpret_cast<const uint2*>(row + swz(x0));
-        v[0] = u.x;
-        v[1] = u.y;
-    } else {
+    for (int t = RB - 1; t >= T0; --t) {
+        const int h = (1 << RB) >> (t + 1);
 #pragma unroll
-        for (int e = 0; e < G; ++e) v[e] = row[swz(x0 + (e << SUB))];
-    }
-    radix_butterflies<RAD, LS0, INV>(v, hi, twf, p);
-    if constexpr (SUB == 0 && RAD >= 2) {
+        for (int m = 0; m < (1 << t); ++m) {
+            const Tw2 w = tw(t, m);
 #pragma unroll
-        for (int q = 0; q < G / 4; ++q)
-            *reinterpret_cast<uint4*>(row + swz(x0 + 4 * q)) = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-    } else if constexpr (SUB == 0 && RAD == 1) {
-        *reinterpret_cast<uint2*>(row + swz(x0)) = make_uint2(v[0], v[1]);
-    } else {
-#pragma unroll
-        for (int e = 0; e < G; ++e) row[swz(x0 + (e << SUB))] = v[e];
-    }
-}
-
-// rows [0, rpb) x 2^NB words between global (contiguous) and shared (swizzled rows),
-// 16-byte vectors, eight in flight per thread.  Requires 2^NB >= 4.
-template <int NB, bool TO_SMEM>
-__device__ __forceinline__ void move_rows(uint32_t* sh, uint32_t* g, int rpb) {
-    constexpr int Q = (1 << NB) / 4;  // vectors per row
-    const int total = rpb * Q;
-    for (int b0 = threadIdx.x; b0 < total; b0 += 8 * blockDim.x) {
-        uint4 v[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int q = b0 + u * blockDim.x;
-            if (q < total) {
-                const int rr = q / Q, x = 4 * (q % Q);
-                v[u] = TO_SMEM ? *reinterpret_cast<const uint4*>(g + 4 * (size_t)q)
-                               : *reinterpret_cast<const uint4*>(sh + (rr << NB) + swz(x));
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int q = b0 + u * blockDim.x;
-            if (q < total) {
-                const int rr = q / Q, x = 4 * (q % Q);
-                if (TO_SMEM) *reinterpret_cast<uint4*>(sh + (rr << NB) + swz(x)) = v[u];
-                else *reinterpret_cast<uint4*>(g + 4 * (size_t)q) = v[u];
-            }
+            for (int i = 0; i < h; ++i) bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
         }
     }
 }
 
-template <int V>
-using IntC = std::integral_constant<int, V>;
-
-// Runs body(IntC<LS0>, IntC<RAD>) for every radix-8 pass of a 2^NB-point line transform
-// (forward: LS0 = 0, 3, 6, ...; inverse: the same passes in reverse), one barrier after each.
-template <int NB, int PI, bool INV, class Body>
-__device__ __forceinline__ void for_each_pass(const Body& body) {
-    constexpr int NPASS = (NB + 2) / 3;
-    if constexpr (PI < NPASS) {
-        constexpr int IDX = INV ? NPASS - 1 - PI : PI;
-        constexpr int LS0 = 3 * IDX;
-        constexpr int RAD = (NB - LS0) < 3 ? (NB - LS0) : 3;
-        body(IntC<LS0>{}, IntC<RAD>{});
-        __syncthreads();
-        for_each_pass<NB, PI + 1, INV>(body);
+// ---------------------------------------------------------------------------------------
+// Row pass layout.  LPR = 2^(NB-RB) threads share a row; a shared-memory region serves
+// GRP = max(32, LPR) threads (one warp, or the two warps of a 1024-point row) and holds
+// RPG = GRP / LPR rows.  Inside a region an element has the index X = (row << NB) | x; it
+// is stored at X ^ G(X >> 5), an XOR swizzle chosen (by exhaustive search over linear maps)
+// so that every exchange of the phase layouts below is free of bank conflicts -- with
+// 16-byte vector access in the last phase for NB = 6, 7, 8.
+// ---------------------------------------------------------------------------------------
+template <int NB>
+struct RowCfg : LineCfg<NB> {
+    using B = LineCfg<NB>;
+    static constexpr int LPR = 1 << (NB - B::RB);
+    static constexpr int GRP = LPR > 32 ? LPR : 32;
+    static constexpr int ROWS_PER_CTA = 128 / LPR;   // 128 threads per CTA
+    static constexpr bool VEC = NB >= 6 && NB <= 8;   // swizzle keeps runs of 4 contiguous
+    __host__ __device__ static constexpr uint32_t g(int i) {
+        // G(input bit i of X >> 5) for each NB; NB <= 4 has a single phase and no exchange
+        return NB == 5 || NB == 9 ? (i == 0 ? 2u : i == 1 ? 4u : i == 2 ? 8u : i == 3 ? 17u : 0u)
+             : NB == 6           ? (i == 0 ? 4u : i == 1 ? 8u : i == 2 ? 4u : i == 3 ? 16u : 0u)
+             : NB == 7           ? (i == 0 ? 4u : i == 1 ? 8u : i == 2 ? 8u : i == 3 ? 16u : 0u)
+             : NB == 8           ? (i == 0 ? 4u : i == 1 ? 8u : i == 2 ? 0u : i == 3 ? 16u : 0u)
+             : NB == 10          ? (i == 0 ? 1u : i == 1 ? 18u : i == 2 ? 4u : i == 3 ? 8u : 0u)
+                                 : 0u;
     }
+    static __device__ __forceinline__ int swz(int X) {
+        const int h = X >> 5;
+        return X ^ ((h & 1 ? (int)g(0) : 0) ^ (h & 2 ? (int)g(1) : 0) ^ (h & 4 ? (int)g(2) : 0) ^
+                    (h & 8 ? (int)g(3) : 0) ^ (h & 16 ? (int)g(4) : 0));
+    }
+};
+
+template <int NB>
+__device__ __forceinline__ void region_sync() {
+    if constexpr (RowCfg<NB>::LPR > 32) __syncthreads();
+    else __syncwarp();
 }
 
-// Copies a tile of `rows` x `tc` words between global (row stride gstride) and shared
-// (dense [rows][tc]); with 16-byte vectors, eight loads in flight per thread before any store.
-template <bool TO_SMEM>
-__device__ __forceinline__ void move_tile(uint32_t* sh, uint32_t* g, int rows, int tc, size_t gstride) {
-    const bool vec = ((tc & 3) == 0) && (((uintptr_t)g & 15) == 0) && ((gstride & 3) == 0);
-    if (vec) {
-        const int q4 = tc >> 2, lq = 31 - __clz(q4);
-        const int total = rows * q4;
-        for (int b0 = threadIdx.x; b0 < total; b0 += 8 * blockDim.x) {
-            uint4 v[8];
+// Element index x (within the row) of register e in phase K for row-lane r.
+template <int NB, int K>
+__device__ __forceinline__ int row_x(int r, int e) {
+    using C = RowCfg<NB>;
+    constexpr int b0 = C::b0(K);
+    return ((r >> b0) << (b0 + C::RB)) | (e << b0) | (r & ((1 << b0) - 1));
+}
+
+// Writes (TO_SMEM) or reads the thread's registers in the layout of phase K.
+template <int NB, int K, bool TO_SMEM>
+__device__ __forceinline__ void row_xchg(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r) {
+    using C = RowCfg<NB>;
+    if constexpr (C::VEC && C::b0(K) == 0) {
+        const int X0 = (rho << NB) | row_x<NB, K>(r, 0);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int idx = b0 + u * blockDim.x;
-                if (idx < total) {
-                    const int r = idx >> lq, c = (idx & (q4 - 1)) << 2;
-                    v[u] = TO_SMEM ? *reinterpret_cast<const uint4*>(g + (size_t)r * gstride + c)
-                                   : reinterpret_cast<const uint4*>(sh)[idx];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int idx = b0 + u * blockDim.x;
-                if (idx < total) {
-                    const int r = idx >> lq, c = (idx & (q4 - 1)) << 2;
-                    if (TO_SMEM) reinterpret_cast<uint4*>(sh)[idx] = v[u];
-                    else *reinterpret_cast<uint4*>(g + (size_t)r * gstride + c) = v[u];
-                }
+        for (int q = 0; q < C::E / 4; ++q) {
+            uint4* a = reinterpret_cast<uint4*>(region + C::swz(X0 + 4 * q));
+            if (TO_SMEM) *a = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            else {
+                const uint4 u = *a;
+                v[4 * q] = u.x;
+                v[4 * q + 1] = u.y;
+                v[4 * q + 2] = u.z;
+                v[4 * q + 3] = u.w;
             }
         }
     } else {
-        for (int idx = threadIdx.x; idx < rows * tc; idx += blockDim.x) {
-            uint32_t* gp = g + (size_t)(idx / tc) * gstride + (idx % tc);
-            if (TO_SMEM) sh[idx] = *gp;
-            else *gp = sh[idx];
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) {
+            uint32_t* a = region + C::swz((rho << NB) | row_x<NB, K>(r, e));
+            if (TO_SMEM) *a = v[e];
+            else v[e] = *a;
         }
     }
 }
 
-// Stages the twiddles of row stages 0..w2-1 for rows [hi0, hi0 + rpb) as Tw2 pairs:
-// twf[rpb (2^ls - 1) + t] = tw[2^(w1+ls) + hi0 2^ls + t]; with MIRROR, the entries of the
-// mirrored rows in reverse: tw[2^(w1+ls) + (nrows - hi0) 2^ls - 1 - t].
-template <bool MIRROR>
-__device__ __forceinline__ void stage_row_twiddles(Tw2* out, const uint32_t* tw, int rpb, int w1, int w2,
-                                                   uint32_t nrows, uint32_t hi0, uint32_t pinv) {
-    if ((rpb & 3) == 0 && w1 + 0 >= 2) {
-        const int total4 = rpb * ((1 << w2) - 1) / 4;  // groups of 4 entries, stage blocks are multiples of 4
-        for (int g0 = threadIdx.x; g0 < total4; g0 += 4 * blockDim.x) {
-            uint4 v[4];
-            int dst[4];
+// global <-> registers in the layout of phase K (rows of nc consecutive words)
+template <int NB, int K, bool LOAD>
+__device__ __forceinline__ void row_global(uint32_t (&v)[RowCfg<NB>::E], uint32_t* row, int r, bool active) {
+    using C = RowCfg<NB>;
+    if (!active) {
+        if (LOAD)
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int g = g0 + u * blockDim.x;
-                dst[u] = -1;
-                if (g < total4) {
-                    const int ls = 31 - __clz(4 * g / rpb + 1);
-                    const int o = rpb * ((1 << ls) - 1), t = 4 * g - o;
-                    const uint32_t s0 = 1u << (w1 + ls);
-                    const uint32_t src = MIRROR ? s0 + ((nrows - hi0) << ls) - 4 - t : s0 + (hi0 << ls) + t;
-                    v[u] = *reinterpret_cast<const uint4*>(tw + src);
-                    dst[u] = o + t;
-                }
-            }
+            for (int e = 0; e < C::E; ++e) v[e] = 0;
+        return;
+    }
+    if constexpr (C::b0(K) == 0 && C::E >= 4) {  // E consecutive words, 16-byte aligned
+        uint4* g = reinterpret_cast<uint4*>(row + row_x<NB, K>(r, 0));
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (dst[u] < 0) continue;
-                uint32_t w[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
-                if (MIRROR) {
-                    const uint32_t t0 = w[0], t1 = w[1];
-                    w[0] = w[3];
-                    w[1] = w[2];
-                    w[2] = t1;
-                    w[3] = t0;
-                }
-                uint4* o4 = reinterpret_cast<uint4*>(out + dst[u]);
-                o4[0] = make_uint4(w[0], w[0] * pinv, w[1], w[1] * pinv);
-                o4[1] = make_uint4(w[2], w[2] * pinv, w[3], w[3] * pinv);
+        for (int q = 0; q < C::E / 4; ++q) {
+            if (LOAD) {
+                const uint4 u = g[q];
+                v[4 * q] = u.x;
+                v[4 * q + 1] = u.y;
+                v[4 * q + 2] = u.z;
+                v[4 * q + 3] = u.w;
+            } else {
+                g[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             }
         }
     } else {
-        for (int ls = 0; ls < w2; ++ls) {
-            const int o = rpb * ((1 << ls) - 1), cnt = rpb << ls;
-            const uint32_t s0 = 1u << (w1 + ls);
-            for (int t = threadIdx.x; t < cnt; t += blockDim.x)
-                out[o + t] = make_tw(tw[MIRROR ? s0 + ((nrows - hi0) << ls) - 1 - t : s0 + (hi0 << ls) + t], pinv);
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) {
+            if (LOAD) v[e] = row[row_x<NB, K>(r, e)];
+            else row[row_x<NB, K>(r, e)] = v[e];
+        }
+    }
+}
+
+// Forward phases K..NPH-1 of a row (registers in the layout of phase K on entry, of phase
+// NPH-1 on exit).  Stage ls of row hi, group gi uses tw[2^(w1+ls) + hi 2^ls + gi].
+template <int NB, int K>
+__device__ __forceinline__ void row_forward(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r,
+                                            const uint32_t* twj, int w1, uint32_t hi, uint32_t p, uint32_t pinv) {
+    using C = RowCfg<NB>;
+    if constexpr (K < C::NPH) {
+        constexpr int b0 = C::b0(K);
+        const uint32_t hip = (uint32_t)(r >> b0);  // index bits above the registers
+        auto tw = [&](int t, int m) {
+            const int ls = C::ls(K, t);
+            return make_tw(__ldg(twj + (1u << (w1 + ls)) + (hi << ls) + ((hip << t) | (uint32_t)m)), pinv);
+        };
+        radix_fwd<C::RB, C::t0(K)>(v, tw, p);
+        if constexpr (K + 1 < C::NPH) {
+            row_xchg<NB, K, true>(v, region, rho, r);
+            region_sync<NB>();
+            row_xchg<NB, K + 1, false>(v, region, rho, r);
+            region_sync<NB>();
+            row_forward<NB, K + 1>(v, region, rho, r, twj, w1, hi, p, pinv);
+        }
+    }
+}
+
+// Inverse phases K down to 0 (registers in the layout of phase K on entry, phase 0 on exit).
+// The inverse twiddle of (ls, hi, gi) is the forward entry of the mirrored row nrows-1-hi at
+// 2^ls - 1 - gi.
+template <int NB, int K>
+__device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r,
+                                            const uint32_t* twj, int w1, uint32_t hi_m, uint32_t p, uint32_t pinv) {
+    using C = RowCfg<NB>;
+    if constexpr (K >= 0) {
+        constexpr int b0 = C::b0(K);
+        const uint32_t hip = (uint32_t)(r >> b0);
+        auto tw = [&](int t, int m) {
+            const int ls = C::ls(K, t);
+            const uint32_t gi = (hip << t) | (uint32_t)m;
+            return make_tw(__ldg(twj + (1u << (w1 + ls)) + (hi_m << ls) + ((1u << ls) - 1u - gi)), pinv);
+        };
+        radix_inv<C::RB, C::t0(K)>(v, tw, p);
+        if constexpr (K > 0) {
+            row_xchg<NB, K, true>(v, region, rho, r);
+            region_sync<NB>();
+            row_xchg<NB, K - 1, false>(v, region, rho, r);
+            region_sync<NB>();
+            row_inverse<NB, K - 1>(v, region, rho, r, twj, w1, hi_m, p, pinv);
         }
     }
 }
 
 }  // namespace
 
-// Column pass: the first w1 = NB stages on a tile of 2^ltc columns x 2^NB rows of prime
-// blockIdx.y, batch blockIdx.z.  Column stage s, group i uses tw[2^s + i] (forward) or
-// tw[2^(s+1) - 1 - i] (inverse); all of them index below nrows.  Consecutive threads take
-// consecutive columns, so a warp's 32 lanes hit 32 banks and share one twiddle.
-template <int NB, bool INV>
-__global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restrict__ R, uint32_t col0, int ltc) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int NR = 1 << NB;
-    const int tc = 1 << ltc;
-    Tw2* tws = reinterpret_cast<Tw2*>(smem_raw);            // [NR]
-    uint32_t* sh = reinterpret_cast<uint32_t*>(tws + NR);   // [NR][tc]
-    const int j = (int)blockIdx.y;
-    const uint32_t p = P.p[j], pinv = P.pinv[j];
-    uint32_t* base = R + ((size_t)blockIdx.z * P.K + j) * P.N + col0 + ((uint32_t)blockIdx.x << ltc);
-    const uint32_t* tw = P.tw + (size_t)j * P.N;
-
-    move_tile<true>(sh, base, NR, tc, P.ncols);
-    for (int k = threadIdx.x; k < NR; k += blockDim.x) tws[k] = make_tw(__ldg(tw + k), pinv);
-    __syncthreads();
-
-    auto twf = [&](int ls, int gi) { return INV ? tws[(2 << ls) - 1 - gi] : tws[(1 << ls) + gi]; };
-    for_each_pass<NB, 0, INV>([&](auto l0, auto rd) {
-        constexpr int LS0 = decltype(l0)::value, RAD = decltype(rd)::value;
-        for (int t = threadIdx.x; t < ((NR >> RAD) << ltc); t += blockDim.x)
-            radix_group<NB, LS0, RAD, INV>(sh + (t & (tc - 1)), tc, t >> ltc, twf, p);
-    });
-    move_tile<false>(sh, base, NR, tc, P.ncols);
-}
-
-// Row pass over `rpb` consecutive rows of prime blockIdx.y, batch blockIdx.z.
+// Row pass over ROWS_PER_CTA consecutive rows of prime blockIdx.y, batch blockIdx.z,
+// 128 threads.
 //   FUSED = false: forward row stages (operand a).
 //   FUSED = true : forward row stages of b, pointwise product with the finished transform of
 //                  a (RA), inverse row stages.  The Montgomery pointwise product leaves a
 //                  factor 2^-32 that the CRT constant crt_c compensates.
-// Row stage ls of row hi, group gi uses tw[2^(w1+ls) + hi 2^ls + gi]; for a block of rows
-// [hi0, hi0 + rpb) those entries are one contiguous run per stage, staged in shared memory
-// as twf[rpb (2^ls - 1) + rr 2^ls + gi].  The inverse twiddle of (hi, gi) is the forward
-// entry of the mirrored row nrows-1-hi at 2^ls-1-gi, staged as twi with the same indexing.
 template <int NB, bool FUSED>
-__global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
-                                                  int rpb) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int w2 = NB, nc = 1 << NB;
-    const int w1 = P.w1;
-    const int ntw = ntt_row_twiddle_slots(rpb, nc);
-    Tw2* twf_s = reinterpret_cast<Tw2*>(smem_raw);
-    Tw2* twi_s = twf_s + ntw;
-    uint32_t* sh = reinterpret_cast<uint32_t*>(twi_s + (FUSED ? ntw : 0));
+__global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA) {
+    using C = RowCfg<NB>;
+    __shared__ __align__(16) uint32_t sh[C::NPH > 1 ? 128 * C::E : 4];
+    const int tid = threadIdx.x;
+    const int li = tid % C::GRP;                 // thread within the shared-memory region
+    const int rho = li / C::LPR, r = li % C::LPR;
+    uint32_t* region = sh + (tid / C::GRP) * (C::GRP * C::E);
+    const uint32_t hi = blockIdx.x * C::ROWS_PER_CTA + (uint32_t)(tid / C::LPR);
+    const bool active = hi < P.nrows;
+    const uint32_t hic = active ? hi : P.nrows - 1;  // keeps twiddle reads in range
     const int j = (int)blockIdx.y;
     const uint32_t p = P.p[j], pinv = P.pinv[j];
-    const uint32_t hi0 = blockIdx.x * (uint32_t)rpb;
-    const size_t off = ((size_t)blockIdx.z * P.K + j) * P.N + (size_t)hi0 * nc;
-    uint32_t* rows = R + off;
-    const uint32_t* tw = P.tw + (size_t)j * P.N;
-    constexpr bool VEC = nc >= 4;
+    const size_t off = ((size_t)blockIdx.z * P.K + j) * P.N + (size_t)hic * (1u << NB);
+    uint32_t* row = R + off;
+    const uint32_t* twj = P.tw + (size_t)j * P.N;
 
-    if constexpr (VEC) move_rows<NB, true>(sh, rows, rpb);
-    else
-        for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) sh[idx] = rows[idx];
-    stage_row_twiddles<false>(twf_s, tw, rpb, w1, w2, P.nrows, hi0, pinv);
-    if (FUSED) stage_row_twiddles<true>(twi_s, tw, rpb, w1, w2, P.nrows, hi0, pinv);
-    __syncthreads();
-
-    for_each_pass<NB, 0, false>([&](auto l0, auto rd) {
-        constexpr int LS0 = decltype(l0)::value, RAD = decltype(rd)::value, LG = NB - RAD;
-        for (int t = threadIdx.x; t < (rpb << LG); t += blockDim.x) {
-            const int rr = t >> LG;
-            auto twf = [&](int ls, int gi) { return twf_s[rpb * ((1 << ls) - 1) + (rr << ls) + gi]; };
-            radix_group_row<NB, LS0, RAD, false>(sh + (rr << NB), t & ((1 << LG) - 1), twf, p);
-        }
-    });
-    if (FUSED) {
-        const uint32_t* arows = RA + off;
-        if constexpr (VEC) {
-            for (int q = threadIdx.x; q < rpb * nc / 4; q += blockDim.x) {
-                const int rr = q / (nc / 4), x = 4 * (q % (nc / 4));
-                const uint4 a4 = *reinterpret_cast<const uint4*>(arows + 4 * (size_t)q);
-                uint4* s4 = reinterpret_cast<uint4*>(sh + (rr << NB) + swz(x));
-                uint4 b4 = *s4;
-                // a in [0, 4p) -> [0, p); Montgomery product (0, 2p)
-                b4.x = mont_mul(red_once(red_once(a4.x, 2 * p), p), b4.x, p, pinv);
-                b4.y = mont_mul(red_once(red_once(a4.y, 2 * p), p), b4.y, p, pinv);
-                b4.z = mont_mul(red_once(red_once(a4.z, 2 * p), p), b4.z, p, pinv);
-                b4.w = mont_mul(red_once(red_once(a4.w, 2 * p), p), b4.w, p, pinv);
-                *s4 = b4;
-            }
-        } else {
-            for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) {
-                const uint32_t a = red_once(red_once(arows[idx], 2 * p), p);
-                sh[idx] = mont_mul(a, sh[idx], p, pinv);
-            }
-        }
-        __syncthreads();
-        for_each_pass<NB, 0, true>([&](auto l0, auto rd) {
-            constexpr int LS0 = decltype(l0)::value, RAD = decltype(rd)::value, LG = NB - RAD;
-            for (int t = threadIdx.x; t < (rpb << LG); t += blockDim.x) {
-                const int rr = t >> LG;
-                auto twf = [&](int ls, int gi) { return twi_s[rpb * ((1 << ls) - 1) + (rr << ls) + gi]; };
-                radix_group_row<NB, LS0, RAD, true>(sh + (rr << NB), t & ((1 << LG) - 1), twf, p);
-            }
-        });
+    uint32_t v[C::E];
+    row_global<NB, 0, true>(v, row, r, active);
+    row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p, pinv);
+    if constexpr (FUSED) {
+        uint32_t a[C::E];
+        row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), true>(a, const_cast<uint32_t*>(RA + off), r, active);
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) v[e] = mont_mul(red_once(red_once(a[e], 2 * p), p), v[e], p, pinv);
+        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p, pinv);
+        row_global<NB, 0, false>(v, row, r, active);
+    } else {
+        row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), false>(v, row, r, active);
     }
-    if constexpr (VEC) move_rows<NB, false>(sh, rows, rpb);
-    else
-        for (int idx = threadIdx.x; idx < rpb * nc; idx += blockDim.x) rows[idx] = sh[idx];
+}
+
+// ---------------------------------------------------------------------------------------
+// Column pass: the first w1 = NB stages on a tile of 2^NB rows x TC = 2^ltc columns of prime
+// blockIdx.y, batch blockIdx.z, 256 threads.  Thread t owns column t % TC and, in each phase,
+// the element groups t / TC + i (256 / TC): a group is the 16 rows that differ in the phase's
+// register bits.  Phase 0 (forward) reads its groups straight from global memory and the last
+// phase writes straight back; the tile in shared memory ([row][TC], a warp touching 32
+// consecutive columns of one row) carries the values between phases.  Column stage s, group
+// i uses tw[2^s + i] (forward) or tw[2^(s+1) - 1 - i] (inverse), staged once per CTA with its
+// Shoup companion.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+template <int NB, bool INV, int K>
+__device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32_t* gbase, size_t gstride, int ltc,
+                                          uint32_t p) {
+    using C = LineCfg<NB>;
+    constexpr int b0 = C::b0(K);
+    constexpr int NGRP = (1 << NB) / C::E;  // groups per column
+    constexpr bool FIRST = INV ? K == C::NPH - 1 : K == 0;
+    constexpr bool LAST = INV ? K == 0 : K == C::NPH - 1;
+    const int tc = 1 << ltc;
+    const int c = threadIdx.x & (tc - 1);
+    const int slots = blockDim.x >> ltc;
+    for (int gidx = threadIdx.x >> ltc; gidx < NGRP; gidx += slots) {
+        const int lo = gidx & ((1 << b0) - 1), hip = gidx >> b0;
+        const int xb = (hip << (b0 + C::RB)) | lo;
+        uint32_t v[C::E];
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) {
+            const int x = xb | (e << b0);
+            v[e] = FIRST ? gbase[(size_t)x * gstride + c] : tile[(x << ltc) + c];
+        }
+        if (!INV) {
+            auto tw = [&](int t, int m) { return tws[(1 << C::ls(K, t)) + ((hip << t) | m)]; };
+            radix_fwd<C::RB, C::t0(K)>(v, tw, p);
+        } else {
+            auto tw = [&](int t, int m) { return tws[(2 << C::ls(K, t)) - 1 - ((hip << t) | m)]; };
+            radix_inv<C::RB, C::t0(K)>(v, tw, p);
+        }
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) {
+            const int x = xb | (e << b0);
+            if (LAST) gbase[(size_t)x * gstride + c] = v[e];
+            else tile[(x << ltc) + c] = v[e];
+        }
+    }
+}
+
+template <int NB, bool INV, int I>
+__device__ __forceinline__ void col_phases(uint32_t* tile, const Tw2* tws, uint32_t* gbase, size_t gstride, int ltc,
+                                           uint32_t p) {
+    using C = LineCfg<NB>;
+    if constexpr (I < C::NPH) {
+        constexpr int K = INV ? C::NPH - 1 - I : I;
+        col_phase<NB, INV, K>(tile, tws, gbase, gstride, ltc, p);
+        if constexpr (I + 1 < C::NPH) {
+            __syncthreads();
+            col_phases<NB, INV, I + 1>(tile, tws, gbase, gstride, ltc, p);
+        }
+    }
+}
+
+}  // namespace
+
+template <int NB, bool INV>
+__global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restrict__ R, uint32_t col0, int ltc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NR = 1 << NB;
+    Tw2* tws = reinterpret_cast<Tw2*>(smem_raw);            // [NR]
+    uint32_t* tile = reinterpret_cast<uint32_t*>(tws + NR);  // [NR][TC]
+    const int j = (int)blockIdx.y;
+    const uint32_t p = P.p[j], pinv = P.pinv[j];
+    uint32_t* base = R + ((size_t)blockIdx.z * P.K + j) * P.N + col0 + ((uint32_t)blockIdx.x << ltc);
+    const uint32_t* tw = P.tw + (size_t)j * P.N;
+    for (int k = threadIdx.x; k < NR; k += blockDim.x) tws[k] = make_tw(__ldg(tw + k), pinv);
+    __syncthreads();
+    col_phases<NB, INV, 0>(tile, tws, base, P.ncols, ltc, p);
 }
 
 namespace {
@@ -390,13 +355,12 @@ void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevP
 }
 
 template <int NB>
-void launch_rows_nb(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
-                    const uint32_t* RA, int rpb) {
-    if (fused) k_ntt_rows<NB, true><<<grid, 128, smem, s>>>(P, R, RA, rpb);
-    else k_ntt_rows<NB, false><<<grid, 128, smem, s>>>(P, R, RA, rpb);
+void launch_rows_nb(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA) {
+    if (fused) k_ntt_rows<NB, true><<<grid, 128, 0, s>>>(P, R, RA);
+    else k_ntt_rows<NB, false><<<grid, 128, 0, s>>>(P, R, RA);
 }
 
-// Applies f<NB>() for the line length nb in [0, PM_MAX_LINE_LOG].
+// Applies F<NB>::run(...) for the line length 2^nb, nb in [0, 10].
 template <template <int> class F, class... A>
 void dispatch_nb(int nb, A&&... a) {
     switch (nb) {
@@ -426,10 +390,9 @@ struct RowsF {
     static void run(A&&... a) { launch_rows_nb<NB>(a...); }
 };
 template <int NB>
-struct AttrF {
+struct ColAttrF {
     static void run(int bytes) {
-        const void* fns[4] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>,
-                              (const void*)k_ntt_rows<NB, false>, (const void*)k_ntt_rows<NB, true>};
+        const void* fns[2] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>};
         for (const void* f : fns) {
             const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
             if (e != cudaSuccess) throw_cuda(e, "NTT kernel attribute");
@@ -437,16 +400,30 @@ struct AttrF {
     }
 };
 template <int NB>
-struct ProbeF {
+struct ColProbeF {
     static void run() {
-        const void* fns[4] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>,
-                              (const void*)k_ntt_rows<NB, false>, (const void*)k_ntt_rows<NB, true>};
+        const void* fns[2] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>};
         for (const void* f : fns) {
             cudaFuncAttributes fa{};
             const cudaError_t e = cudaFuncGetAttributes(&fa, f);
             if (e != cudaSuccess) throw_cuda(e, "NTT kernel image");
         }
     }
+};
+template <int NB>
+struct RowProbeF {
+    static void run() {
+        const void* fns[2] = {(const void*)k_ntt_rows<NB, false>, (const void*)k_ntt_rows<NB, true>};
+        for (const void* f : fns) {
+            cudaFuncAttributes fa{};
+            const cudaError_t e = cudaFuncGetAttributes(&fa, f);
+            if (e != cudaSuccess) throw_cuda(e, "NTT kernel image");
+        }
+    }
+};
+template <int NB>
+struct RowsPerCtaF {
+    static void run(int* out) { *out = RowCfg<NB>::ROWS_PER_CTA; }
 };
 
 }  // namespace
@@ -456,28 +433,28 @@ void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const Dev
     dispatch_nb<ColsF>(P.w1, inv, grid, smem, s, P, R, col0, ltc);
 }
 
-void launch_ntt_rows(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
-                     const uint32_t* RA, int rpb) {
-    dispatch_nb<RowsF>(P.w2, fused, grid, smem, s, P, R, RA, rpb);
+void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA) {
+    dispatch_nb<RowsF>(P.w2, fused, grid, s, P, R, RA);
+}
+
+int ntt_rows_per_cta(int w2) {
+    int r = 0;
+    dispatch_nb<RowsPerCtaF>(w2, &r);
+    return r;
 }
 
 void ntt_set_smem_limit(int bytes, int w1, int w2) {
-    dispatch_nb<AttrF>(w1, bytes);
-    if (w2 != w1) dispatch_nb<AttrF>(w2, bytes);
+    (void)w2;  // the row kernels use static shared memory only
+    if (w1 > 0) dispatch_nb<ColAttrF>(w1, bytes);
 }
 
 void ntt_probe_images(int w1, int w2) {
-    dispatch_nb<ProbeF>(w1);
-    if (w2 != w1) dispatch_nb<ProbeF>(w2);
+    if (w1 > 0) dispatch_nb<ColProbeF>(w1);
+    dispatch_nb<RowProbeF>(w2);
 }
 
 size_t ntt_cols_smem(const DevPlan& P, int ltc) {
     return (size_t)P.nrows * sizeof(Tw2) + ((size_t)P.nrows << ltc) * 4;
-}
-
-size_t ntt_rows_smem(const DevPlan& P, int rpb, bool fused) {
-    const size_t ntw = (size_t)ntt_row_twiddle_slots(rpb, (int)P.ncols);
-    return ntw * sizeof(Tw2) * (fused ? 2 : 1) + (size_t)rpb * P.ncols * 4;
 }
 
 }  // namespace pm

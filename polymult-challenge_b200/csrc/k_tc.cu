@@ -292,7 +292,8 @@ __global__ void __launch_bounds__(256, 1) k_rns_tc(DevPlan P, const uint32_t* __
 // ----------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256, 1) k_crt_tc(DevPlan P, const uint32_t* __restrict__ R, ChunkMap C,
                                                    uint32_t npos, uint32_t nbatch, uint32_t* __restrict__ out,
-                                                   int use_bulk) {
+                                                   int gather) {
+    const bool use_bulk = gather == CRT_GATHER_BULK;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int K = P.K, KP = P.KP, L = P.L, kb = P.crt_kbytes, nrows_b = P.crt_nrows;
     const int zl = crt_zl(L), zs = crt_zstride(L);
@@ -367,6 +368,16 @@ __global__ void __launch_bounds__(256, 1) k_crt_tc(DevPlan P, const uint32_t* __
         const bool valid = m < cnt;
         if (use_bulk) {
             ok = ok && mbar_wait_bounded(bar_r, i & 1);
+        } else if (gather == CRT_GATHER_VEC) {
+            // runs of 4 positions are 4 consecutive residues (cw, col0 multiples of 4): one
+            // 16-byte load per prime and run, spread over all 256 threads
+            const uint32_t* Rb = R + (size_t)b * K * P.N;
+            for (int idx = threadIdx.x; idx < K * (TC_M / 4); idx += blockDim.x) {
+                const int j = idx / (TC_M / 4), q4 = 4 * (idx % (TC_M / 4));
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (q4 < cnt) v = *reinterpret_cast<const uint4*>(Rb + (size_t)j * P.N + chunk_pos_to_n(P, C, pos0 + q4));
+                *reinterpret_cast<uint4*>(rt + (size_t)j * TC_M + q4) = v;
+            }
         } else if (hf == 0) {
             const uint32_t* Rb = R + (size_t)b * K * P.N;
             const uint32_t n = valid ? chunk_pos_to_n(P, C, pos0 + m) : 0;

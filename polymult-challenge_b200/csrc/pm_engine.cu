@@ -245,6 +245,7 @@ Engine::~Engine() {
     for (auto e : ev_done_in_) cudaEventDestroy(e);
     for (auto e : ev_crt_) cudaEventDestroy(e);
     for (auto e : ev_out_) cudaEventDestroy(e);
+    for (auto e : trace_ev_) cudaEventDestroy(e);
     if (ev_row_a_) cudaEventDestroy(ev_row_a_);
     if (ev_fused_) cudaEventDestroy(ev_fused_);
     for (auto s : s_comp_)
@@ -298,11 +299,9 @@ void Engine::upload_tables() {
 }
 
 void Engine::setup_launch_shapes() {
-    rpb_ = (int)std::min<uint32_t>(plan_.nrows, std::max<uint32_t>(1, 1024 / plan_.ncols));
+    rpb_ = ntt_rows_per_cta(plan_.w2);
     smem_cols_ = ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(32, plan_.ncols)));
-    smem_rows_fwd_ = ntt_rows_smem(dp_, rpb_, false);
-    smem_rows_fused_ = ntt_rows_smem(dp_, rpb_, true);
-    if (smem_cols_ > smem_optin_ || smem_rows_fused_ > smem_optin_) throw Unsupported("NTT tile exceeds shared memory");
+    if (smem_cols_ > smem_optin_) throw Unsupported("NTT tile exceeds shared memory");
     dec_tab_smem_ = rns_plain_smem(dp_, true) <= 100 * 1024;
     smem_dec_ = rns_plain_smem(dp_, dec_tab_smem_);
     smem_crt_ = crt_plain_smem(dp_);
@@ -356,6 +355,10 @@ void Engine::setup_host_pipeline() {
     cuda_check(cudaHostAlloc(&h_status_, 16, cudaHostAllocDefault), "cudaHostAlloc");
     *h_status_ = 0;
     profile_ = std::getenv("POLYMULT_PROFILE") != nullptr;
+    if (profile_) {
+        trace_ev_.resize(8 + 2 * 2 * cin_.size() + 2 * cout_.size());
+        for (auto& e : trace_ev_) cuda_check(cudaEventCreate(&e), "event");
+    }
     for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
@@ -411,8 +414,8 @@ void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStrea
 }
 
 void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s) const {
-    dim3 grid(plan_.nrows / rpb_, plan_.K, nb);
-    launch_ntt_rows(fused, grid, fused ? smem_rows_fused_ : smem_rows_fwd_, s, dp_, R, RA, rpb_);
+    dim3 grid((plan_.nrows + rpb_ - 1) / rpb_, plan_.K, nb);
+    launch_ntt_rows(fused, grid, s, dp_, R, RA);
     cuda_check(cudaGetLastError(), fused ? "launch k_ntt_rows<fused>" : "launch k_ntt_rows<forward>");
 }
 
@@ -421,8 +424,9 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
     if (form_ == GEMM_TENSOR) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
-        const int bulk = ch.cw >= 4 && ch.col0 % 4 == 0 && plan_.N % 4 == 0 && ((uintptr_t)R % 16 == 0);
-        k_crt_tc<<<grid, CRT_TC_THREADS, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out, bulk);
+        const bool vec = ch.cw >= 4 && ch.col0 % 4 == 0 && plan_.N % 4 == 0 && ((uintptr_t)R % 16 == 0);
+        const int gather = !vec ? CRT_GATHER_SCALAR : ch.cw >= 32 ? CRT_GATHER_BULK : CRT_GATHER_VEC;
+        k_crt_tc<<<grid, CRT_TC_THREADS, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out, gather);
         cuda_check(cudaGetLastError(), "launch k_crt_tc");
     } else {
         dim3 grid((npos + CRT_TM - 1) / CRT_TM, 1, nb);
@@ -568,6 +572,14 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     const auto t0 = clk::now();
     auto us = [&](clk::time_point t) { return std::chrono::duration<double, std::micro>(t - t0).count(); };
     clk::time_point t_stage0, t_inputs, t_first_out, t_last_out;
+    // POLYMULT_PROFILE: device timeline from timing events on the pipeline's streams
+    std::vector<std::pair<std::string, cudaEvent_t>> marks;
+    auto mark = [&](const std::string& name, cudaStream_t st) {
+        if (!profile_ || marks.size() >= trace_ev_.size()) return;
+        cuda_check(cudaEventRecord(trace_ev_[marks.size()], st), "record");
+        marks.emplace_back(name, trace_ev_[marks.size()]);
+    };
+    mark("start", s_h2d_);
     stage(0);
     t_stage0 = clk::now();
     for (int i = 0; i < nin; ++i) {
@@ -577,14 +589,17 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         cudaStream_t sc = s_comp_[i % 3];
         cuda_check(cudaMemcpyAsync(d_in_[P] + off, h_in_[P] + off, words * 4, cudaMemcpyHostToDevice, s_h2d_), "H2D");
         cuda_check(cudaEventRecord(ev_in_[i], s_h2d_), "record");
+        mark("h2d" + std::to_string(i), s_h2d_);
         cuda_check(cudaStreamWaitEvent(sc, ev_in_[i], 0), "wait");
         launch_dec(d_in_[P] + off, ch, 1, dR[P], sc);
         launch_cols(false, dR[P], ch, 1, sc);
         cuda_check(cudaEventRecord(ev_done_in_[i], sc), "record");
+        mark("in" + std::to_string(i), sc);
         if (i == na - 1) {  // a complete: its row pass overlaps b's transfer
             for (int k = 0; k < na; ++k) cuda_check(cudaStreamWaitEvent(s_comp_[0], ev_done_in_[k], 0), "wait");
             launch_rows(false, d_ra_, nullptr, 1, s_comp_[0]);
             cuda_check(cudaEventRecord(ev_row_a_, s_comp_[0]), "record");
+            mark("rowA", s_comp_[0]);
         }
         if (i + 1 < nin) stage(i + 1);
     }
@@ -593,6 +608,7 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     for (int k = na; k < nin; ++k) cuda_check(cudaStreamWaitEvent(s0, ev_done_in_[k], 0), "wait");
     launch_rows(true, d_rb_, d_ra_, 1, s0);
     cuda_check(cudaEventRecord(ev_fused_, s0), "record");
+    mark("fused", s0);
     for (size_t oc = 0; oc < cout_.size(); ++oc) {
         const Chunk ch = cout_[oc];
         const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
@@ -601,9 +617,11 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         launch_cols(true, d_rb_, ch, 1, sc);
         launch_crt(d_rb_, ch, 1, d_out_ + off, sc);
         cuda_check(cudaEventRecord(ev_crt_[oc], sc), "record");
+        mark("crt" + std::to_string(oc), sc);
         cuda_check(cudaStreamWaitEvent(s_d2h_, ev_crt_[oc], 0), "wait");
         cuda_check(cudaMemcpyAsync(h_out_ + off, d_out_ + off, words * 4, cudaMemcpyDeviceToHost, s_d2h_), "D2H");
         cuda_check(cudaEventRecord(ev_out_[oc], s_d2h_), "record");
+        mark("d2h" + std::to_string(oc), s_d2h_);
     }
     // device status word -> pinned memory behind the last D2H (s_d2h has waited on every CRT)
     cuda_check(cudaMemcpyAsync(h_status_, dp_.status, 4, cudaMemcpyDeviceToHost, s_d2h_), "status D2H");
@@ -624,10 +642,21 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
                 stream_copy(c + ((size_t)r * ncols + ch.col0) * L, srcc + r * seg, seg * 4);
         });
     }
-    if (profile_)
+    if (profile_) {
         std::fprintf(stderr,
-                     "polymult: stage0 %.1f us | inputs issued %.1f | first out %.1f | last out %.1f | done %.1f\n",
+                     "polymult: host: stage0 %.1f us | inputs issued %.1f | first out %.1f | last out %.1f | done %.1f\n",
                      us(t_stage0), us(t_inputs), us(t_first_out), us(t_last_out), us(clk::now()));
+        std::string line = "polymult: device (us after start):";
+        for (size_t k = 1; k < marks.size(); ++k) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, marks[0].second, marks[k].second) == cudaSuccess) {
+                char buf[64];
+                std::snprintf(buf, sizeof buf, " %s %.1f", marks[k].first.c_str(), 1000.0 * ms);
+                line += buf;
+            }
+        }
+        std::fprintf(stderr, "%s\n", line.c_str());
+    }
     const uint32_t st = *h_status_;
     if (st) {
         *h_status_ = 0;

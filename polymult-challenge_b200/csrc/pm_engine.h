@@ -133,7 +133,7 @@ class Engine {
 
     // launch shapes
     int rpb_ = 1;
-    size_t smem_cols_ = 0, smem_rows_fwd_ = 0, smem_rows_fused_ = 0;
+    size_t smem_cols_ = 0;
     size_t smem_dec_ = 0, smem_crt_ = 0;
     bool dec_tab_smem_ = false;
 
@@ -147,7 +147,8 @@ class Engine {
     cudaStream_t s_h2d_ = nullptr, s_d2h_ = nullptr;
     std::vector<cudaEvent_t> ev_in_, ev_done_in_, ev_crt_, ev_out_;
     uint32_t* h_status_ = nullptr;  // pinned copy of the device status word, written after each run_host
-    bool profile_ = false;          // POLYMULT_PROFILE: per-call host phase timeline on stderr
+    bool profile_ = false;          // POLYMULT_PROFILE: per-call host and device timeline on stderr
+    std::vector<cudaEvent_t> trace_ev_;  // timing events of that timeline
     cudaEvent_t ev_row_a_ = nullptr, ev_fused_ = nullptr;
     std::unique_ptr<HostPool> pool_;
 };

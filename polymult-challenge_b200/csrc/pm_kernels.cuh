@@ -18,19 +18,13 @@ namespace pm {
 // no module registered); these host wrappers are the interface.
 void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
                      int ltc);
-void launch_ntt_rows(bool fused, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R,
-                     const uint32_t* RA, int rpb);
+void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA);
+// rows of 2^w2 words per row-pass CTA (grid.x = ceil(nrows / this))
+int ntt_rows_per_cta(int w2);
 // line lengths 2^w1 (columns) and 2^w2 (rows) select the compile-time specialisations
 void ntt_set_smem_limit(int bytes, int w1, int w2);  // max dynamic shared memory of their kernels
 void ntt_probe_images(int w1, int w2);              // throws CudaError if an image cannot load
 size_t ntt_cols_smem(const DevPlan& P, int ltc);
-// Tw2 slots per twiddle array of a row-pass CTA: rpb (ncols - 1), at least 1, rounded up to
-// even so that the row tile that follows the arrays starts 16-byte aligned
-__host__ __device__ inline int ntt_row_twiddle_slots(int rpb, int ncols) {
-    const int n = rpb * (ncols - 1);
-    return ((n > 0 ? n : 1) + 1) & ~1;
-}
-size_t ntt_rows_smem(const DevPlan& P, int rpb, bool fused);
 
 // ---- plain (CUDA-core) RNS decomposition and CRT (k_rns.cu)
 constexpr int DEC_TM = 64;   // coefficients per decomposition block
@@ -45,7 +39,11 @@ constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
 __global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R,
                          int use_bulk);
 __global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
-                         int use_bulk);
+                         int gather);
+// how k_crt_tc gathers a tile's residues: per-prime bulk copies of whole 128-byte row
+// segments (chunks >= 32 columns), 16-byte loads by every thread (narrower chunks of a
+// multiple of 4 columns), or 4-byte loads
+enum : int { CRT_GATHER_SCALAR = 0, CRT_GATHER_VEC = 1, CRT_GATHER_BULK = 2 };
 constexpr int RNS_TC_THREADS = 256;  // 8 epilogue warps: 4 TMEM lane quarters x 2 prime halves
 constexpr int CRT_TC_THREADS = 256;  // two threads per coefficient / TMEM lane
 size_t rns_tc_smem(const DevPlan& P);
