@@ -57,6 +57,16 @@ def parse():
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the uneven-batch leg")
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=10000)
+    ap.add_argument("--serve-plain-requests", type=int, default=3000)
+    ap.add_argument("--serve-rate", type=float, default=2500.0)
+    ap.add_argument("--serve-batch", type=int, default=8)
+    ap.add_argument("--serve-streams", type=int, default=4)
+    ap.add_argument("--serve-pool", type=int, default=64)
     return ap.parse_args()
 
 
@@ -272,6 +282,166 @@ def time_device(torch, m, da, db, dc, batch, steps, warm):
     return e0.elapsed_time(e1)
 
 
+BATCH_NS = (4096, 8192, 16384, 32768, 65536)
+BATCH_WS = (256, 868, 1747, 3000)
+
+
+def batched_workload(count=256, seed=4):
+    """The uneven batch: `count` multiplications, N and W drawn from a seed; grouped into
+    classes of one point each.  Returns [(N, W, count)], sorted by (N, W)."""
+    import random
+    rng = random.Random(seed)
+    draws = [(rng.choice(BATCH_NS), rng.choice(BATCH_WS)) for _ in range(count)]
+    cls = {}
+    for nw in draws:
+        cls[nw] = cls.get(nw, 0) + 1
+    return [(N, W, c) for (N, W), c in sorted(cls.items())]
+
+
+def run_batched(torch, args, local):
+    """256 uneven multiplications: one CUDA-graph launch per step (autotuned split and GEMM
+    form per class) vs the same multiplications as sequential single calls of the plain form."""
+    import numpy as np
+    import polymult
+    import workload
+    classes = batched_workload(args.batch_count)
+    stream = torch.cuda.current_stream()
+    ks = []
+    for i, (N, W, c) in enumerate(classes):
+        q = workload.spec_prime(N, W)
+        L = (W + 31) // 32
+        ops = workload.uniform_operands(N, W, q, 2 * c, seed=9000 + i)
+        da = torch.from_numpy(np.ascontiguousarray(ops[:c]).view(np.int32)).cuda()
+        db = torch.from_numpy(np.ascontiguousarray(ops[c:]).view(np.int32)).cuda()
+        ks.append({"N": N, "W": W, "L": L, "q": q, "count": c, "a": da, "b": db, "c": torch.zeros_like(da)})
+    total = sum(k["count"] for k in ks)
+    spec = [(k["N"], k["W"], workload.limbs(k["q"], k["L"]), k["count"], k["a"].data_ptr(), k["b"].data_ptr(),
+             k["c"].data_ptr()) for k in ks]
+
+    def time_batch(b, steps, warm):
+        for _ in range(warm):
+            b.run(stream.cuda_stream)
+        b.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            b.run(stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        b.sync()
+        return e0.elapsed_time(e1) / steps
+
+    out = {"workload": "%d multiplications, N from %s, W from %s (seeded), %d classes, operands in HBM"
+                       % (total, list(BATCH_NS), list(BATCH_WS), len(ks)), "classes": len(ks)}
+    tune_cache = os.environ.get("POLYMULT_TUNE_CACHE")
+    with polymult.Batch(spec, tune=True, device=local) as b:
+        ms = time_batch(b, args.batch_steps, 3)
+        inf = b.info()
+        chosen = [b.class_info(i) for i in range(len(ks))]
+    with polymult.Batch(spec, tune=False, device=local) as b:
+        ms_default = time_batch(b, args.batch_steps, 3)
+    # the same multiplications as sequential single calls of the plain form
+    mults = []
+    for k in ks:
+        m = polymult.Multiplier(k["N"], k["W"], workload.limbs(k["q"], k["L"]), gemm="plain", device=local)
+        mults.append(m)
+    cw = [k["N"] * k["L"] for k in ks]
+
+    def seq_once():
+        for k, m, w in zip(ks, mults, cw):
+            for i in range(k["count"]):
+                m.multiply_device(k["a"].data_ptr() + 4 * w * i, k["b"].data_ptr() + 4 * w * i,
+                                  k["c"].data_ptr() + 4 * w * i, 1, stream.cuda_stream)
+    seq_once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    seq_once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_seq = e0.elapsed_time(e1)
+    for m in mults:
+        m.sync()
+    # spot check: batch outputs (last written by the sequential plain calls) equal the graph's
+    ref = [k["c"].clone() for k in ks]
+    with polymult.Batch(spec, tune=True, device=local) as b:
+        b.run(stream.cuda_stream)
+        b.sync()
+    same = all(bool(torch.equal(k["c"], r)) for k, r in zip(ks, ref))
+    for m in mults:
+        m.close()
+    forms = {}
+    for c in chosen:
+        forms[c["gemm"]] = forms.get(c["gemm"], 0) + 1
+    out.update({"value": round(total / (ms / 1000.0), 2), "unit": "mults/s", "ms_per_batch": round(ms, 4),
+                "untuned_value": round(total / (ms_default / 1000.0), 2),
+                "sequential_plain_value": round(total / (ms_seq / 1000.0), 2),
+                "speedup_vs_sequential_plain": round(ms_seq / ms, 3),
+                "graph_nodes": inf["graph_nodes"], "kernel_launches": inf["kernel_launches"],
+                "streams": inf["streams"], "scratch_gb": round(inf["scratch_bytes"] / 1e9, 3),
+                "gemm_forms_chosen": forms, "splits_chosen": sorted({(c["w1"], c["w2"]) for c in chosen}),
+                "matches_sequential_plain": same, "tune_cache": tune_cache or "default"})
+    return out
+
+
+def run_serving(args, local):
+    """Poisson stream of requests at N=65536 W=1747, each multiplying a fresh operand by one of
+    8 operands resident in NTT form; continuous batching under a 150 GB HBM budget vs the
+    unbatched plain path (one request at a time, CUDA-core GEMMs) on the same stream."""
+    import numpy as np
+    import polymult
+    import workload
+    N, W = N_RANK, W_RANK
+    L = (W + 31) // 32
+    q = workload.spec_prime(N, W)
+    qv = workload.limbs(q, L)
+    res = workload.uniform_operands(N, W, q, 8, seed=77)
+    pool = args.serve_pool
+    ops = workload.uniform_operands(N, W, q, pool, seed=78)
+    n = args.serve_requests
+    rng = np.random.default_rng(79)
+    t = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=n))
+    t -= t[0]
+    sel = rng.integers(0, 8, size=n).astype(np.uint32)
+    src = rng.integers(0, pool, size=n)
+    out = {"workload": "%d requests, Poisson arrivals at %.0f/s (seeded), N=%d W=%d, 8 resident operands in NTT form, "
+                       "request operands from a pool of %d pinned buffers" % (n, args.serve_rate, N, W, pool),
+           "hbm_budget_gb": 150}
+
+    def leg(max_batch, streams, gemm, n_req):
+        with polymult.Server(N, W, qv, res, hbm_budget=150 * 10**9, max_batch=max_batch, streams=streams, gemm=gemm,
+                             device=local) as srv:
+            a = srv.pinned(pool)
+            a[:] = ops
+            c = srv.pinned(pool)
+            lat, st = srv.run(t[:n_req], sel[:n_req], [a[i] for i in src[:n_req]], [c[i] for i in src[:n_req]])
+            # results of requests whose output buffer no later request reused, against the single path
+            last = {}
+            for i in range(n_req):
+                last[int(src[i])] = i
+            check = sorted(last.values())[-4:]
+            got = {i: np.array(c[src[i]]) for i in check}
+        lat_ms = np.sort(lat) * 1000.0
+        return {"p50_ms": round(float(np.percentile(lat_ms, 50)), 3), "p99_ms": round(float(np.percentile(lat_ms, 99)), 3),
+                "mean_ms": round(float(lat_ms.mean()), 3), "throughput": round(n_req / st["seconds"], 2),
+                "batches": st["batches"], "mean_batch": round(st["mean_batch"], 2),
+                "peak_inflight": st["peak_inflight"], "max_inflight_by_budget": st["max_inflight"],
+                "requests": n_req}, got
+
+    served, got = leg(args.serve_batch, args.serve_streams, "auto", n)
+    ok = True
+    with polymult.Multiplier(N, W, qv, device=local) as m:
+        for i, c in got.items():
+            want = m.multiply(ops[src[i]], res[sel[i]])
+            ok = ok and bool(np.array_equal(c, want))
+    plain, _ = leg(1, 1, "plain", min(n, args.serve_plain_requests))
+    out.update({"continuous_batching": served, "unbatched_plain": plain, "unit": "requests/s",
+                "results_match_single_path": ok,
+                "p99_ratio_plain_over_batched": round(plain["p99_ms"] / served["p99_ms"], 2),
+                "throughput_ratio": round(served["throughput"] / plain["throughput"], 2)})
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -359,6 +529,14 @@ def run_ours(args):
            "pcie_gbs": {k: round(v, 2) for k, v in bw.items()}, "pcie_floor_ms": round(floor_ms, 4),
            "p50_over_floor": round(lat_ms[len(lat_ms) // 2] / floor_ms, 3)}
 
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(torch, args, local)
+
+    serving = None
+    if not args.no_serving:
+        serving = run_serving(args, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu, cref = reference_cpu(N, W, q, a0, b0, calls=1, warm=0)
@@ -379,7 +557,8 @@ def run_ours(args):
                 "forms_agree": forms_agree,
                 "stages_ms": {k: round(v, 4) for k, v in stages.items()},
                 "stages_ms_plain": {k: round(v, 4) for k, v in stages_plain.items()},
-                "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "roofline": roofline, "e2e": e2e, "batched": batched, "serving": serving, "cpu_baseline": cpu,
+                "clocks": clk.summary(),
                 "gpu_launches": launches}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -104,6 +104,93 @@ int pm_time_stages(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, ui
  * capture.  The context must come from an earlier pm_init (which does allocate). */
 int pm_run_device_static(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream);
 
+/* ---- Batches of multiplications of uneven points.  No reference counterpart: the reference
+ * multiplies one pair per fherma_run call (solve.cu:1480-1498) with fixed split and chunking
+ * heuristics (solve.cu:85-87, 917-918, 1403-1419).
+ *
+ * A batch is a list of classes, each one point (N, W, q) and `count` multiplications of it
+ * whose operands lie contiguously in device memory.  pm_batch_init builds every class's
+ * tables, allocates the residue scratch once, and captures the whole schedule -- one launch
+ * per kernel per class, classes spread over up to 8 streams -- into a CUDA graph;
+ * pm_batch_run replays it with one graph launch.  The operand pointers are captured: write
+ * new inputs into the same buffers between runs.  With PM_BATCH_TUNE the 4-step split and
+ * the GEMM form of each class are chosen by timing the candidates on the class's operands
+ * (results cached in $POLYMULT_TUNE_CACHE, default ~/.cache/polymult_b200/tune.txt); the
+ * tuning runs write the outputs.  Results are bit-identical whatever the choice. */
+typedef struct pm_batch pm_batch;
+
+typedef struct pm_batch_class {
+    uint32_t N, W, L;
+    const uint32_t* q;   /* host memory, L limbs (copied by pm_batch_init) */
+    uint32_t count;      /* multiplications of this point (0 allowed) */
+    const uint32_t* d_a; /* device memory, [count][N][L] */
+    const uint32_t* d_b; /* device memory, [count][N][L] */
+    uint32_t* d_c;       /* device memory, [count][N][L] */
+    int32_t w1;          /* 4-step split nrows = 2^w1 (both line lengths <= 2^10); -1: default or tuned */
+} pm_batch_class;
+
+enum pm_batch_flags {
+    PM_BATCH_TUNE = 1,     /* measure and choose split and GEMM form per class */
+    PM_BATCH_NO_GRAPH = 2  /* launch the schedule directly on every run instead of a graph */
+};
+
+typedef struct pm_batch_info {
+    uint32_t classes;
+    uint32_t streams;        /* streams the classes are spread over */
+    int32_t kernel_launches; /* kernels per run */
+    uint64_t graph_nodes;    /* nodes of the captured graph (0 with PM_BATCH_NO_GRAPH) */
+    uint64_t scratch_bytes;  /* device residue scratch of the batch */
+} pm_batch_info;
+
+typedef struct pm_batch_class_info {
+    int32_t K, w1, w2;
+    int32_t gemm_form;  /* PM_GEMM_PLAIN or PM_GEMM_TENSOR */
+    double tuned_ms;    /* measured ms of the chosen configuration; 0 untuned, -1 from the cache */
+} pm_batch_class_info;
+
+int pm_batch_init(const pm_batch_class* classes, uint32_t nclasses, int gemm_form, int flags, int device,
+                  pm_batch** out);
+/* Asynchronous on `stream` (NULL = legacy default stream); pm_batch_sync waits. */
+int pm_batch_run(pm_batch* batch, void* stream);
+/* Waits for the batch's device work; PM_ERR_DEVICE if a device-side check failed. */
+int pm_batch_sync(pm_batch* batch);
+int pm_batch_get_info(const pm_batch* batch, pm_batch_info* out);
+int pm_batch_get_class(const pm_batch* batch, uint32_t index, pm_batch_class_info* out);
+void pm_batch_free(pm_batch* batch);
+
+/* ---- Serving.  No reference counterpart (the reference serves one fherma_run call at a time,
+ * main.cpp:181-186).  A server holds one point and `nresident` fixed operands, uploaded once and
+ * kept on the device in NTT form (decomposed and forward-transformed).  pm_server_run plays a
+ * stream of requests: request i arrives t_arrive[i] seconds after the call starts and asks for
+ * c[i] = a[i] * resident[sel[i]] (a[i], c[i]: host buffers of N*L words; pinned ones from
+ * pm_server_host_alloc let the copies run asynchronously).  Continuous batching: whenever one of
+ * the server's `streams` slots is free, it takes every queued request up to its capacity,
+ * whatever their resident operand, and runs them as one batch while other slots' batches are on
+ * the GPU.  Admission: each request in flight holds 8NL + 4KN bytes of device memory; with the
+ * resident transforms and tables, the total stays within hbm_budget bytes.  Each result is
+ * bit-identical to the same multiplication run alone.  Synchronous; fills latency[i] (seconds,
+ * completion - arrival) and *stats. */
+typedef struct pm_server pm_server;
+
+typedef struct pm_serve_stats {
+    uint64_t requests;
+    uint64_t batches;
+    double mean_batch;       /* requests per launched batch */
+    uint32_t peak_inflight;  /* most requests in flight at once */
+    uint32_t max_inflight;   /* the admission limit the budget gives */
+    double seconds;          /* first arrival to last completion */
+} pm_serve_stats;
+
+int pm_server_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const uint32_t* resident, uint32_t nresident,
+                   uint64_t hbm_budget, uint32_t max_batch, uint32_t streams, int gemm_form, int device,
+                   pm_server** out);
+int pm_server_run(pm_server* server, uint32_t n, const double* t_arrive, const uint32_t* sel,
+                  const uint32_t* const* a, uint32_t* const* c, double* latency, pm_serve_stats* stats);
+/* Pinned host memory owned by the server (freed by pm_server_free if not before). */
+int pm_server_host_alloc(pm_server* server, size_t bytes, void** out);
+int pm_server_host_free(pm_server* server, void* p);
+void pm_server_free(pm_server* server);
+
 /* Waits for the context's device work and returns PM_ERR_DEVICE if a device-side check
  * failed since the last call. */
 int pm_sync(pm_context* ctx);

@@ -233,9 +233,12 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
 //   FUSED = false: forward row stages (operand a).
 //   FUSED = true : forward row stages of b, pointwise product with the finished transform of
 //                  a (RA), inverse row stages.  The Montgomery pointwise product leaves a
-//                  factor 2^-32 that the CRT constant crt_c compensates.
+//                  factor 2^-32 that the CRT constant crt_c compensates.  Batch z pairs with
+//                  transform ra_sel[z] of RA when ra_sel is given (a server's resident
+//                  operands), else with transform z.
 template <int NB, bool FUSED>
-__global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA) {
+__global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
+                                                  const uint32_t* __restrict__ ra_sel) {
     using C = RowCfg<NB>;
     __shared__ __align__(16) uint32_t sh[C::NPH > 1 ? 128 * C::E : 4];
     const int tid = threadIdx.x;
@@ -256,7 +259,9 @@ __global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restric
     row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p, pinv);
     if constexpr (FUSED) {
         uint32_t a[C::E];
-        row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), true>(a, const_cast<uint32_t*>(RA + off), r, active);
+        const size_t za = ra_sel ? (size_t)__ldg(ra_sel + blockIdx.z) : (size_t)blockIdx.z;
+        const size_t offa = (za * P.K + j) * P.N + (size_t)hic * (1u << NB);
+        row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), true>(a, const_cast<uint32_t*>(RA + offa), r, active);
 #pragma unroll
         for (int e = 0; e < C::E; ++e) v[e] = mont_mul(red_once(red_once(a[e], 2 * p), p), v[e], p, pinv);
         row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p, pinv);
@@ -355,9 +360,10 @@ void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevP
 }
 
 template <int NB>
-void launch_rows_nb(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA) {
-    if (fused) k_ntt_rows<NB, true><<<grid, 128, 0, s>>>(P, R, RA);
-    else k_ntt_rows<NB, false><<<grid, 128, 0, s>>>(P, R, RA);
+void launch_rows_nb(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
+                    const uint32_t* ra_sel) {
+    if (fused) k_ntt_rows<NB, true><<<grid, 128, 0, s>>>(P, R, RA, ra_sel);
+    else k_ntt_rows<NB, false><<<grid, 128, 0, s>>>(P, R, RA, ra_sel);
 }
 
 // Applies F<NB>::run(...) for the line length 2^nb, nb in [0, 10].
@@ -433,8 +439,9 @@ void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const Dev
     dispatch_nb<ColsF>(P.w1, inv, grid, smem, s, P, R, col0, ltc);
 }
 
-void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA) {
-    dispatch_nb<RowsF>(P.w2, fused, grid, s, P, R, RA);
+void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
+                     const uint32_t* ra_sel) {
+    dispatch_nb<RowsF>(P.w2, fused, grid, s, P, R, RA, ra_sel);
 }
 
 int ntt_rows_per_cta(int w2) {

@@ -123,6 +123,94 @@ int pm_get_info(const pm_context* ctx, pm_info* out) {
     return PM_OK;
 }
 
+int pm_batch_init(const pm_batch_class* classes, uint32_t nclasses, int gemm_form, int flags, int device,
+                  pm_batch** out) {
+    if (!out) return fail(PM_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!classes || nclasses == 0) return fail(PM_ERR_INVALID, "no classes");
+    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_TENSOR) return fail(PM_ERR_INVALID, "bad gemm_form");
+    if (flags & ~(PM_BATCH_TUNE | PM_BATCH_NO_GRAPH)) return fail(PM_ERR_INVALID, "unknown flags");
+    return guarded([&] { *out = new pm_batch{new pm::Batch(classes, nclasses, gemm_form, flags, device)}; });
+}
+
+int pm_batch_run(pm_batch* batch, void* stream) {
+    if (!batch || !batch->batch) return fail(PM_ERR_INVALID, "null batch");
+    return guarded([&] { batch->batch->run(static_cast<cudaStream_t>(stream)); });
+}
+
+int pm_batch_sync(pm_batch* batch) {
+    if (!batch || !batch->batch) return fail(PM_ERR_INVALID, "null batch");
+    return guarded([&] { batch->batch->sync(); });
+}
+
+int pm_batch_get_info(const pm_batch* batch, pm_batch_info* out) {
+    if (!batch || !batch->batch || !out) return fail(PM_ERR_INVALID, "null argument");
+    const pm::Batch& b = *batch->batch;
+    std::memset(out, 0, sizeof *out);
+    out->classes = (uint32_t)b.classes();
+    out->streams = (uint32_t)b.streams();
+    out->kernel_launches = b.kernel_launches();
+    out->graph_nodes = b.graph_nodes();
+    out->scratch_bytes = b.scratch_bytes();
+    return PM_OK;
+}
+
+int pm_batch_get_class(const pm_batch* batch, uint32_t index, pm_batch_class_info* out) {
+    if (!batch || !batch->batch || !out) return fail(PM_ERR_INVALID, "null argument");
+    const pm::Batch& b = *batch->batch;
+    if (index >= b.classes()) return fail(PM_ERR_INVALID, "class index out of range");
+    const pm::Engine& e = b.engine(index);
+    std::memset(out, 0, sizeof *out);
+    out->K = e.plan().K;
+    out->w1 = e.plan().w1;
+    out->w2 = e.plan().w2;
+    out->gemm_form = e.gemm_form();
+    out->tuned_ms = b.tuned_ms(index);
+    return PM_OK;
+}
+
+void pm_batch_free(pm_batch* batch) {
+    if (!batch) return;
+    delete batch->batch;
+    delete batch;
+}
+
+int pm_server_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const uint32_t* resident, uint32_t nresident,
+                   uint64_t hbm_budget, uint32_t max_batch, uint32_t streams, int gemm_form, int device,
+                   pm_server** out) {
+    if (!out) return fail(PM_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (!resident || nresident == 0) return fail(PM_ERR_INVALID, "no resident operands");
+    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_TENSOR) return fail(PM_ERR_INVALID, "bad gemm_form");
+    return guarded([&] {
+        *out = new pm_server{
+            new pm::Server(N, W, L, q, resident, nresident, hbm_budget, max_batch, streams, gemm_form, device)};
+    });
+}
+
+int pm_server_run(pm_server* server, uint32_t n, const double* t_arrive, const uint32_t* sel,
+                  const uint32_t* const* a, uint32_t* const* c, double* latency, pm_serve_stats* stats) {
+    if (!server || !server->server) return fail(PM_ERR_INVALID, "null server");
+    if (n && (!t_arrive || !sel || !a || !c || !latency)) return fail(PM_ERR_INVALID, "null argument");
+    return guarded([&] { server->server->run(n, t_arrive, sel, a, c, latency, stats); });
+}
+
+int pm_server_host_alloc(pm_server* server, size_t bytes, void** out) {
+    if (!server || !server->server || !out) return fail(PM_ERR_INVALID, "null argument");
+    return guarded([&] { *out = server->server->host_alloc(bytes); });
+}
+
+int pm_server_host_free(pm_server* server, void* p) {
+    if (!server || !server->server) return fail(PM_ERR_INVALID, "null server");
+    return guarded([&] { server->server->host_free(p); });
+}
+
+void pm_server_free(pm_server* server) {
+    if (!server) return;
+    delete server->server;
+    delete server;
+}
+
 const char* pm_last_error(void) { return g_last_error.c_str(); }
 
 int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int32_t* K_out) {

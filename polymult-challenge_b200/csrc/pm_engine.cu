@@ -201,8 +201,10 @@ T* dev_upload(std::vector<void*>& keep, const std::vector<T>& v, size_t* total) 
 // ---------------------------------------------------------------------------------------
 // construction
 // ---------------------------------------------------------------------------------------
-Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_request, int device)
+Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_request, int device,
+               const EngineOptions& opt)
     : plan_(make_plan(N, W, L, q)), device_(device) {
+    if (opt.w1 >= 0) set_split(plan_, opt.w1);
     int ndev = 0;
     cuda_check(cudaGetDeviceCount(&ndev), "no CUDA device");
     if (device < 0 || device >= ndev) throw CudaError("device index out of range");
@@ -228,8 +230,10 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
         // one multiply's worth of residues per group at the ranked size; more for small N
         const size_t per_mult = (size_t)plan_.K * plan_.N;
         group_cap_ = (uint32_t)std::max<size_t>(1, std::min<size_t>(256, (8u << 20) / std::max<size_t>(1, per_mult)));
-        ensure_scratch(1);
-        setup_host_pipeline();
+        if (opt.host_pipeline) {
+            ensure_scratch(1);
+            setup_host_pipeline();
+        }
     } catch (...) {
         for (void* d : dev_allocs_) cudaFree(d);
         dev_allocs_.clear();
@@ -413,9 +417,10 @@ void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStrea
     cuda_check(cudaGetLastError(), inv ? "launch k_ntt_cols<inverse>" : "launch k_ntt_cols<forward>");
 }
 
-void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s) const {
+void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s,
+                         const uint32_t* ra_sel) const {
     dim3 grid((plan_.nrows + rpb_ - 1) / rpb_, plan_.K, nb);
-    launch_ntt_rows(fused, grid, s, dp_, R, RA);
+    launch_ntt_rows(fused, grid, s, dp_, R, RA, ra_sel);
     cuda_check(cudaGetLastError(), fused ? "launch k_ntt_rows<fused>" : "launch k_ntt_rows<forward>");
 }
 
@@ -511,15 +516,21 @@ void Engine::time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint
 void Engine::run_device_with_scratch(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* ra, uint32_t* rb,
                                      cudaStream_t s) {
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    run_group(a, b, c, 1, ra, rb, s);
+}
+
+void Engine::run_group(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t nb, uint32_t* ra, uint32_t* rb,
+                       cudaStream_t s) const {
+    if (nb == 0) return;
     const Chunk all{0, plan_.ncols};
-    launch_dec(a, all, 1, ra, s);
-    launch_cols(false, ra, all, 1, s);
-    launch_rows(false, ra, nullptr, 1, s);
-    launch_dec(b, all, 1, rb, s);
-    launch_cols(false, rb, all, 1, s);
-    launch_rows(true, rb, ra, 1, s);
-    launch_cols(true, rb, all, 1, s);
-    launch_crt(rb, all, 1, c, s);
+    launch_dec(a, all, nb, ra, s);
+    launch_cols(false, ra, all, nb, s);
+    launch_rows(false, ra, nullptr, nb, s);
+    launch_dec(b, all, nb, rb, s);
+    launch_cols(false, rb, all, nb, s);
+    launch_rows(true, rb, ra, nb, s);
+    launch_cols(true, rb, all, nb, s);
+    launch_crt(rb, all, nb, c, s);
     cuda_check(cudaGetLastError(), "kernel launch");
 }
 

@@ -68,9 +68,16 @@ struct Chunk {
     uint32_t col0, cw;
 };
 
+// Construction options beyond the point itself.
+struct EngineOptions {
+    bool host_pipeline = true;  // pinned staging + streams for run_host (not needed by batches)
+    int w1 = -1;                // 4-step split nrows = 2^w1 (-1: logN / 2)
+};
+
 class Engine {
   public:
-    Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_request, int device);
+    Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_request, int device,
+           const EngineOptions& opt = EngineOptions());
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
@@ -82,6 +89,10 @@ class Engine {
     // allocates nothing.  Asynchronous on `stream`.
     void run_device_with_scratch(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* ra, uint32_t* rb,
                                  cudaStream_t stream);
+    // nb multiplies in one launch per kernel, residue scratch supplied by the caller (two
+    // arrays of nb*K*N words); allocates nothing and may be captured in a CUDA graph.
+    void run_group(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t nb, uint32_t* ra, uint32_t* rb,
+                   cudaStream_t stream) const;
     // Per-kernel mean durations (ms) of `reps` groups of `count` multiplies (CUDA events).
     void time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t count, int reps, cudaStream_t s,
                      float* ms_out);
@@ -105,7 +116,8 @@ class Engine {
     // launch helpers (also used by the tests' stage-by-stage checks)
     void launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s) const;
     void launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s) const;
-    void launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s) const;
+    void launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s,
+                     const uint32_t* ra_sel = nullptr) const;
     void launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s) const;
 
   private:

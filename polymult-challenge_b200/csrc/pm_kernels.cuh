@@ -18,7 +18,9 @@ namespace pm {
 // no module registered); these host wrappers are the interface.
 void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
                      int ltc);
-void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA);
+// fused: batch z of R pairs with transform ra_sel[z] of RA (ra_sel == nullptr: transform z)
+void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
+                     const uint32_t* ra_sel = nullptr);
 // rows of 2^w2 words per row-pass CTA (grid.x = ceil(nrows / this))
 int ntt_rows_per_cta(int w2);
 // line lengths 2^w1 (columns) and 2^w2 (rows) select the compile-time specialisations

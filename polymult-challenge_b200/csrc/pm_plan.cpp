@@ -387,4 +387,15 @@ std::string check_plan(const Plan& P) {
     return "";
 }
 
+void set_split(Plan& P, int w1) {
+    const int w2 = P.logN - w1;
+    if (w1 < 0 || w2 < 0 || w1 > 10 || w2 > 10 || (P.logN > 0 && w2 < 1))
+        throw InvalidPoint("4-step split out of range: w1 = " + std::to_string(w1) + " for logN = " +
+                           std::to_string(P.logN));
+    P.w1 = w1;
+    P.w2 = w2;
+    P.nrows = 1u << w1;
+    P.ncols = 1u << w2;
+}
+
 }  // namespace pm

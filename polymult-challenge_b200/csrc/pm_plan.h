@@ -73,6 +73,11 @@ struct Plan {
 // Builds every table. Throws InvalidPoint for a malformed point.
 Plan make_plan(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q);
 
+// Changes the 4-step split to nrows = 2^w1, ncols = 2^(logN - w1).  The tables do not
+// depend on the split (twiddles are indexed by the bit-reversed stage position), so any
+// w1 with both line lengths in [1, 2^10] gives the same transform.  Throws InvalidPoint.
+void set_split(Plan& P, int w1);
+
 // Offset in bytes of element (row, kbyte) inside a K-major no-swizzle canonical tile
 // whose rows hold k_bytes bytes.
 inline size_t umma_kmajor_offset(int row, int kbyte, int k_bytes) {

@@ -47,6 +47,30 @@ class PmInfo(ctypes.Structure):
                 ("group", ctypes.c_int32)]
 
 
+class PmBatchClass(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_uint32), ("W", ctypes.c_uint32), ("L", ctypes.c_uint32),
+                ("q", ctypes.c_void_p), ("count", ctypes.c_uint32), ("d_a", ctypes.c_void_p),
+                ("d_b", ctypes.c_void_p), ("d_c", ctypes.c_void_p), ("w1", ctypes.c_int32)]
+
+
+class PmBatchInfo(ctypes.Structure):
+    _fields_ = [("classes", ctypes.c_uint32), ("streams", ctypes.c_uint32),
+                ("kernel_launches", ctypes.c_int32), ("graph_nodes", ctypes.c_uint64),
+                ("scratch_bytes", ctypes.c_uint64)]
+
+
+class PmBatchClassInfo(ctypes.Structure):
+    _fields_ = [("K", ctypes.c_int32), ("w1", ctypes.c_int32), ("w2", ctypes.c_int32),
+                ("gemm_form", ctypes.c_int32), ("tuned_ms", ctypes.c_double)]
+
+
+BATCH_TUNE, BATCH_NO_GRAPH = 1, 2
+
+
+class PmServeStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("mean_batch", ctypes.c_double),
+                ("peak_inflight", ctypes.c_uint32), ("max_inflight", ctypes.c_uint32), ("seconds", ctypes.c_double)]
+
 _lib: Optional[ctypes.CDLL] = None
 
 
@@ -90,6 +114,31 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_plan_selfcheck.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp,
                                       ctypes.POINTER(ctypes.c_int32)]
     lib.pm_plan_selfcheck.restype = ctypes.c_int
+    lib.pm_batch_init.argtypes = [ctypes.POINTER(PmBatchClass), ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.POINTER(vp)]
+    lib.pm_batch_init.restype = ctypes.c_int
+    lib.pm_batch_run.argtypes = [vp, vp]
+    lib.pm_batch_run.restype = ctypes.c_int
+    lib.pm_batch_sync.argtypes = [vp]
+    lib.pm_batch_sync.restype = ctypes.c_int
+    lib.pm_batch_get_info.argtypes = [vp, ctypes.POINTER(PmBatchInfo)]
+    lib.pm_batch_get_info.restype = ctypes.c_int
+    lib.pm_batch_get_class.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(PmBatchClassInfo)]
+    lib.pm_batch_get_class.restype = ctypes.c_int
+    lib.pm_batch_free.argtypes = [vp]
+    lib.pm_batch_free.restype = None
+    lib.pm_server_init.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp, vp, ctypes.c_uint32,
+                                   ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(vp)]
+    lib.pm_server_init.restype = ctypes.c_int
+    lib.pm_server_run.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.POINTER(PmServeStats)]
+    lib.pm_server_run.restype = ctypes.c_int
+    lib.pm_server_host_alloc.argtypes = [vp, ctypes.c_size_t, ctypes.POINTER(vp)]
+    lib.pm_server_host_alloc.restype = ctypes.c_int
+    lib.pm_server_host_free.argtypes = [vp, vp]
+    lib.pm_server_host_free.restype = ctypes.c_int
+    lib.pm_server_free.argtypes = [vp]
+    lib.pm_server_free.restype = None
     del u32p
     _lib = lib
     return lib
@@ -165,6 +214,131 @@ class Multiplier:
     def close(self):
         if getattr(self, "_h", None):
             load().pm_free(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Multiplications of uneven points in one CUDA-graph launch (pm_batch_*).
+
+    classes: sequence of (N, W, q_limbs, count, a_ptr, b_ptr, c_ptr[, w1]) -- device operands
+    [count][N][L] each, w1 an explicit 4-step split (default -1: logN/2, or tuned).
+    tune=True lets the autotuner choose split and GEMM form per class.
+    """
+
+    def __init__(self, classes, gemm: str = "auto", tune: bool = False, graph: bool = True, device: int = 0):
+        lib = load()
+        n = len(classes)
+        arr = (PmBatchClass * n)()
+        self._q = []
+        for i, cls in enumerate(classes):
+            N, W, q_limbs, count, a, b, c = cls[:7]
+            w1 = int(cls[7]) if len(cls) > 7 else -1
+            L = (int(W) + 31) // 32
+            q = _u32(q_limbs)
+            if q.size != L:
+                raise RuntimeError("q must have L limbs")
+            self._q.append(q)
+            arr[i] = PmBatchClass(int(N), int(W), L, q.ctypes.data, int(count), a or None, b or None, c or None,
+                                  w1)
+        flags = (BATCH_TUNE if tune else 0) | (0 if graph else BATCH_NO_GRAPH)
+        h = ctypes.c_void_p()
+        _check(lib.pm_batch_init(arr, n, GEMM_FORMS[gemm], flags, device, ctypes.byref(h)))
+        self._h = h
+
+    def run(self, stream: int = 0):
+        _check(load().pm_batch_run(self._h, stream or None))
+
+    def sync(self):
+        _check(load().pm_batch_sync(self._h))
+
+    def info(self) -> dict:
+        inf = PmBatchInfo()
+        _check(load().pm_batch_get_info(self._h, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in PmBatchInfo._fields_}
+
+    def class_info(self, i: int) -> dict:
+        inf = PmBatchClassInfo()
+        _check(load().pm_batch_get_class(self._h, i, ctypes.byref(inf)))
+        d = {f: getattr(inf, f) for f, _ in PmBatchClassInfo._fields_}
+        d["gemm"] = GEMM_NAMES.get(d["gemm_form"], "?")
+        return d
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pm_batch_free(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving loop with continuous batching over resident operands (pm_server_*).
+
+    resident: (R, N, L) u32 host array of the fixed operands, kept on the device in NTT form.
+    """
+
+    def __init__(self, N: int, W: int, q_limbs, resident, hbm_budget: int = 150 * 10**9, max_batch: int = 8,
+                 streams: int = 4, gemm: str = "auto", device: int = 0):
+        lib = load()
+        self.N, self.W = int(N), int(W)
+        self.L = (self.W + 31) // 32
+        q = _u32(q_limbs)
+        res = np.ascontiguousarray(resident, dtype=np.uint32)
+        if res.ndim != 3 or res.shape[1:] != (self.N, self.L):
+            raise RuntimeError("resident operands must have shape (R, N, L)")
+        h = ctypes.c_void_p()
+        _check(lib.pm_server_init(self.N, self.W, self.L, q.ctypes.data, res.ctypes.data, res.shape[0],
+                                  int(hbm_budget), max_batch, streams, GEMM_FORMS[gemm], device, ctypes.byref(h)))
+        self._h = h
+        self.nresident = res.shape[0]
+
+    def pinned(self, count: int) -> np.ndarray:
+        """(count, N, L) u32 array in pinned host memory owned by the server."""
+        nbytes = count * self.N * self.L * 4
+        p = ctypes.c_void_p()
+        _check(load().pm_server_host_alloc(self._h, nbytes, ctypes.byref(p)))
+        buf = (ctypes.c_uint32 * (count * self.N * self.L)).from_address(p.value)
+        return np.ctypeslib.as_array(buf).reshape(count, self.N, self.L)
+
+    def run(self, t_arrive, sel, a_bufs, c_bufs):
+        """Plays the request stream; a_bufs[i] / c_bufs[i] are (N, L) u32 host arrays.
+        Returns (latency seconds per request, stats dict)."""
+        n = len(t_arrive)
+        t = np.ascontiguousarray(t_arrive, dtype=np.float64)
+        sv = np.ascontiguousarray(sel, dtype=np.uint32)
+        ap = (ctypes.c_void_p * n)(*[x.ctypes.data for x in a_bufs])
+        cp = (ctypes.c_void_p * n)(*[x.ctypes.data for x in c_bufs])
+        lat = np.zeros(n, dtype=np.float64)
+        st = PmServeStats()
+        _check(load().pm_server_run(self._h, n, t.ctypes.data, sv.ctypes.data, ap, cp, lat.ctypes.data,
+                                    ctypes.byref(st)))
+        return lat, {f: getattr(st, f) for f, _ in PmServeStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().pm_server_free(self._h)
             self._h = None
 
     def __enter__(self):

@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """One device-resident multiply group at a chosen point, for profiling under ncu.
 
-    python polymult-challenge_b200/profile_case.py [--N 65536] [--W 1747] [--gemm tensor] [--count 1]
+    python polymult-challenge_b200/profile_case.py [--N 65536] [--W 1747] [--gemm tensor] [--count 1] [--host 0]
 
 pm_init runs one warm-up multiply through the chunked host pipeline first (the input
 column chunks launch the decomposition and column-pass kernels once per chunk, the output
@@ -9,6 +9,8 @@ chunks the inverse column pass and CRT once per chunk; the row passes launch onc
 this script runs `count` multiplies through pm_run_device and checks the device status.
 Select the device-resident launch of a kernel with ncu's -k / -s (skip the warm-up launches):
     ncu --set full --clock-control none -k regex:k_crt_tc -s 20 -c 1 python .../profile_case.py
+--host H then runs H multiplies through pm_run (host operands, the chunked PCIe pipeline);
+with POLYMULT_PROFILE=1 in the environment each call prints its host and device timeline.
 """
 import argparse
 import os
@@ -23,6 +25,7 @@ def main():
     ap.add_argument("--W", type=int, default=1747)
     ap.add_argument("--gemm", default="tensor")
     ap.add_argument("--count", type=int, default=1)
+    ap.add_argument("--host", type=int, default=0)
     a = ap.parse_args()
     import numpy as np
     import torch
@@ -39,6 +42,14 @@ def main():
         m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), a.count,
                           torch.cuda.current_stream().cuda_stream)
         m.sync()
+        if a.host:
+            a0 = np.ascontiguousarray(ops[0])
+            b0 = np.ascontiguousarray(ops[a.count])
+            out = np.empty((a.N, L), dtype=np.uint32)
+            for _ in range(a.host):
+                m.multiply(a0, b0, out)
+            if not np.array_equal(out, dc[0].cpu().numpy().view(np.uint32)):
+                raise SystemExit("host and device paths differ")
     print("ok N=%d W=%d K=%d gemm=%s count=%d input chunks/operand=%s" % (
         a.N, a.W, info["K"], info["gemm"], a.count, "see pm_info"))
 
