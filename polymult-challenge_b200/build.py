@@ -5,7 +5,9 @@
 
 Every .cu / .cpp under csrc/ is compiled with
     -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -Xptxas -v
-and linked (shared cudart) into polymult-challenge_b200/lib/libpolymult_b200.so.  The ptxas
+and linked (shared cudart) into polymult-challenge_b200/lib/libpolymult_b200.so; the
+point-directory runner runner/polymult_solution.cpp is linked against it into
+lib/polymult_solution.  The ptxas
 resource report (registers, spills, shared memory per kernel) goes to lib/ptxas.log.
 """
 import argparse
@@ -19,6 +21,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libpolymult_b200.so")
+RUNNER_SRC = os.path.join(HERE, "runner", "polymult_solution.cpp")
+RUNNER = os.path.join(LIBDIR, "polymult_solution")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -52,8 +56,10 @@ def compile_one(src, verbose):
 def up_to_date():
     if not os.path.exists(LIB):
         return False
-    t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) < t for f in sources() + headers() + [__file__])
+    if not os.path.exists(RUNNER):
+        return False
+    t = min(os.path.getmtime(LIB), os.path.getmtime(RUNNER))
+    return all(os.path.getmtime(f) < t for f in sources() + headers() + [__file__, RUNNER_SRC])
 
 
 def build(force=False, verbose=False):
@@ -74,6 +80,14 @@ def build(force=False, verbose=False):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))
+    # the point-directory runner, linked against the library (found next to it at run time)
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(HERE, "..", "include"), RUNNER_SRC, "-o", RUNNER,
+           "-L" + LIBDIR, "-lpolymult_b200", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath,/usr/local/cuda/lib64"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("runner build failed:\n%s%s" % (r.stdout, r.stderr))
     return LIB
 
 

@@ -376,8 +376,10 @@ void Engine::setup_host_pipeline() {
     mk(ev_out_, cout_.size());
     cuda_check(cudaEventCreateWithFlags(&ev_row_a_, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
-    // 8 copying threads saturate this class of host's memory bandwidth; more only contend
-    pool_.reset(new HostPool(std::max(0, std::min(7, usable_cpus() - 2))));
+    // 8 copying threads (7 workers + the caller) by default; POLYMULT_HOST_THREADS overrides
+    int workers = std::max(0, std::min(7, usable_cpus() - 2));
+    if (const char* e = std::getenv("POLYMULT_HOST_THREADS")) workers = std::max(0, std::min(63, std::atoi(e) - 1));
+    pool_.reset(new HostPool(workers));
 }
 
 int Engine::kernel_launches_per_group() const { return plan_.w1 > 0 ? 8 : 6; }
@@ -585,6 +587,7 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     clk::time_point t_stage0, t_inputs, t_first_out, t_last_out;
     // POLYMULT_PROFILE: device timeline from timing events on the pipeline's streams
     std::vector<std::pair<std::string, cudaEvent_t>> marks;
+    std::vector<double> staged_us;  // host time each input chunk finished staging
     auto mark = [&](const std::string& name, cudaStream_t st) {
         if (!profile_ || marks.size() >= trace_ev_.size()) return;
         cuda_check(cudaEventRecord(trace_ev_[marks.size()], st), "record");
@@ -612,7 +615,10 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
             cuda_check(cudaEventRecord(ev_row_a_, s_comp_[0]), "record");
             mark("rowA", s_comp_[0]);
         }
-        if (i + 1 < nin) stage(i + 1);
+        if (i + 1 < nin) {
+            stage(i + 1);
+            if (profile_) staged_us.push_back(us(clk::now()));
+        }
     }
     cudaStream_t s0 = s_comp_[0];
     cuda_check(cudaStreamWaitEvent(s0, ev_row_a_, 0), "wait");
@@ -667,6 +673,13 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
             }
         }
         std::fprintf(stderr, "%s\n", line.c_str());
+        std::string st = "polymult: host staging done (us):";
+        for (double t : staged_us) {
+            char buf[32];
+            std::snprintf(buf, sizeof buf, " %.1f", t);
+            st += buf;
+        }
+        std::fprintf(stderr, "%s\n", st.c_str());
     }
     const uint32_t st = *h_status_;
     if (st) {
