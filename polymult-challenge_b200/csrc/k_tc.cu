@@ -282,195 +282,287 @@ __global__ void __launch_bounds__(256, 1) k_rns_tc(DevPlan P, const uint32_t* __
 }
 
 // ----------------------------------------------------------------------------------------
-// CRT.  Persistent; 256 threads, two per coefficient: warp w serves TMEM lane quarter w % 4
-// (coefficient m = 32 (w % 4) + lane) and half h = w / 4 of the work -- half of the prime
-// groups in the prologue, half of the result limbs in the epilogue (each half runs its own
-// carry chain; half 0's carry-out is then added into half 1's limbs).  The residues of the
-// next tile arrive by bulk copies into one staging tile while this tile's MMA and epilogue run.
-// smem: [B image][A tile (z rows after the MMA)][R tile K x 128][per-prime constants]
-//       [partial sums 2 x 128][bars][slot]
+// CRT.  Persistent, warp-specialised, 512 threads:
+//   producers (warps 0-7, two threads per coefficient m = t % 128, each half of the prime
+//     groups): load the tile's residues straight from global memory, y_j = x_j (M/p_j)^-1
+//     mod p_j into registers, fp32 partial sums of y_j / p_j; then wait until the previous
+//     tile's MMA has read the A tile, write the y bytes as the K-major A operand, and one
+//     thread issues the tile's MMAs into TMEM accumulator i % 2 (N = result bytes,
+//     K = 4 KP bytes) and commits them;
+//   epilogue (warps 8-15, two threads per coefficient, TMEM lane quarter warp % 4): for tile
+//     i, wait for its accumulator, v = round(sum y_j / p_j), accumulator bytes -> limbs with
+//     carries + T_v into a staging row, release the accumulator, carry merge, delta fold,
+//     - q, coalesced store.
+// With two accumulators the epilogue of tile i overlaps the loads, prologue and MMA of tile
+// i + 1.  Hand-offs: mbarriers mma_done[2] (tcgen05.commit), acc_empty[2] (256 epilogue
+// arrivals), v_ready[2] (one producer arrival after the producers' barrier, releasing the
+// partial sums); named barriers 1 (producers) and 2 (epilogue).  Every wait is bounded: a
+// wait that runs out sets a shared abort flag that ends both loops (agreed per group with a
+// barrier reduction), the status word gets DEV_ERR_WAIT, and the kernel waits (bounded) for
+// its own copies and MMAs in flight before it frees TMEM.
+// smem: [B image][A tile][z staging 128 x zs][per-prime constants KP x uint4]
+//       [partial sums 2 x 2 x 128 f32][bars: b, mma_done 2, acc_empty 2, v_ready 2][slot][abort]
 // ----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 1) k_crt_tc(DevPlan P, const uint32_t* __restrict__ R, ChunkMap C,
-                                                   uint32_t npos, uint32_t nbatch, uint32_t* __restrict__ out,
-                                                   int gather) {
-    const bool use_bulk = gather == CRT_GATHER_BULK;
+namespace {
+
+constexpr int CRT_PROD_THREADS = 256;
+constexpr int CRT_EPI_THREADS = 256;
+constexpr int CRT_MAX_HALF_GROUPS = 16;  // KP <= 128: 4 KP / 16 <= 32 groups of 4 primes, 16 per half
+
+__device__ __forceinline__ void named_sync(int id, int n) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Barrier over `n` threads on named barrier `id`; true if any participant passed p = true.
+__device__ __forceinline__ bool named_sync_or(int id, int n, bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred ip, op;\n\t"
+        "setp.ne.u32 ip, %1, 0;\n\t"
+        "barrier.red.or.pred op, %2, %3, ip;\n\t"
+        "selp.u32 %0, 1, 0, op;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(id), "r"(n)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Bounded wait that also gives up once another thread has set *abort; sets *abort itself
+// when its own limit (about one second of clocks) runs out.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort) return false;
+        if (clock64() - t0 > 2000000000ll) {
+            *abort = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+struct CrtSmem {
+    unsigned char* b;
+    unsigned char* a;
+    uint32_t* z;
+    uint4* cst;
+    float* spart;
+    uint64_t* bars;
+    uint32_t* slot;
+    volatile int* abort;
+};
+
+__host__ __device__ inline size_t crt_z_bytes(const DevPlan& P) { return (size_t)TC_M * crt_zstride(P.L) * 4; }
+
+__device__ __forceinline__ CrtSmem crt_smem(unsigned char* base, const DevPlan& P) {
+    CrtSmem m;
+    m.b = base;
+    m.a = m.b + (size_t)P.crt_nrows * P.crt_kbytes;
+    m.z = reinterpret_cast<uint32_t*>(m.a + (size_t)TC_M * P.crt_kbytes);
+    m.cst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(m.z) + crt_z_bytes(P));
+    m.spart = reinterpret_cast<float*>(m.cst + P.KP);
+    m.bars = reinterpret_cast<uint64_t*>(m.spart + 4 * TC_M);
+    m.slot = reinterpret_cast<uint32_t*>(m.bars + 7);
+    m.abort = reinterpret_cast<volatile int*>(m.slot + 1);
+    return m;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const uint32_t* __restrict__ R, ChunkMap C,
+                                                              uint32_t npos, uint32_t nbatch,
+                                                              uint32_t* __restrict__ out) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    const CrtSmem S = crt_smem(smem_raw, P);
+    uint64_t *bar_b = S.bars, *mma_done = S.bars + 1, *acc_empty = S.bars + 3, *v_ready = S.bars + 5;
     const int K = P.K, KP = P.KP, L = P.L, kb = P.crt_kbytes, nrows_b = P.crt_nrows;
     const int zl = crt_zl(L), zs = crt_zstride(L);
-    unsigned char* b_s = smem_raw;
-    unsigned char* a_s = b_s + (size_t)nrows_b * kb;
-    uint32_t* z_s = reinterpret_cast<uint32_t*>(a_s);            // after the MMA has consumed A
-    uint32_t* rt = reinterpret_cast<uint32_t*>(a_s + crt_a_bytes(P));  // [K][128] (rows >= K never read)
-    uint32_t* cp = rt + (size_t)K * TC_M;                         // p_j
-    uint32_t* cc = cp + KP;                                       // crt_c_j
-    uint32_t* ccc = cc + KP;                                      // crt_cc_j
-    float* crc = reinterpret_cast<float*>(ccc + KP);              // 1 / p_j
-    float* spart = crc + KP;                                      // [2][128]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(spart + 2 * TC_M);
-    uint64_t *bar_b = bars, *bar_r = bars + 1, *bar_mma = bars + 2;
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 3);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int hf = warp >> 2, m = (warp & 3) * 32 + lane;
-    const uint32_t ncols = tmem_cols_for(nrows_b);
+    const uint32_t AS = tmem_cols_for(nrows_b);     // columns per accumulator (<= 256)
     const uint32_t tiles_per_batch = (npos + TC_M - 1) / TC_M;
     const uint32_t ntiles = tiles_per_batch * nbatch;
-    const uint32_t seg = min(C.cw, (uint32_t)TC_M);  // positions per contiguous segment
-    const int kgroups = kb / 16;
-    const int gh = (kgroups + 1) / 2;                 // prime groups of half 0
-    const int nl = nrows_b / 4;                       // limbs covered by the accumulator columns
-    const int lh = ((nl + 1) / 2 + 3) / 4 * 4;        // limbs of half 0 (multiple of 4: 16 columns)
-
-    // warp 0: bulk copies of tile `t`'s residues into rt
-    auto issue_r = [&](uint32_t t) {
-        const uint32_t b = t / tiles_per_batch;
-        const uint32_t pos0 = (t - b * tiles_per_batch) * TC_M;
-        const uint32_t cnt = min((uint32_t)TC_M, npos - pos0);
-        const uint32_t nseg = (cnt + seg - 1) / seg;
-        if (lane == 0) mbar_arrive_expect_tx(bar_r, (uint32_t)K * cnt * 4u);
-        __syncwarp();
-        const uint32_t* Rb = R + (size_t)b * K * P.N;
-        for (uint32_t c = lane; c < (uint32_t)K * nseg; c += 32) {
-            const uint32_t j = c / nseg, sg = c - j * nseg;
-            const uint32_t p0 = pos0 + sg * seg;
-            const uint32_t len = min(seg, pos0 + cnt - p0);
-            bulk_g2s(rt + (size_t)j * TC_M + sg * seg, Rb + (size_t)j * P.N + chunk_pos_to_n(P, C, p0), len * 4, bar_r);
-        }
-    };
+    const uint32_t sbo = 8u * (uint32_t)kb;
 
     if (threadIdx.x == 0) {
-        for (int k = 0; k < 3; ++k) mbar_init(bars + k, 1);
-        bulk_g2s_all(b_s, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
+        mbar_init(bar_b, 1);
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(mma_done + k, 1);
+            mbar_init(acc_empty + k, CRT_EPI_THREADS);
+            mbar_init(v_ready + k, 1);
+        }
+        *S.abort = 0;
+        bulk_g2s_all(S.b, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
     }
-    for (int j = threadIdx.x; j < KP; j += blockDim.x) {
-        cp[j] = P.p[j];
-        cc[j] = P.crt_c[j];
-        ccc[j] = P.crt_cc[j];
-        crc[j] = P.rcp[j];
-    }
-    __syncthreads();
-    if (warp == 0) {
-        if (use_bulk && blockIdx.x < ntiles) issue_r(blockIdx.x);
-        tmem_alloc(slot, ncols);
-    }
+    for (int j = threadIdx.x; j < KP; j += blockDim.x)
+        S.cst[j] = make_uint4(P.p[j], P.crt_c[j], P.crt_cc[j], __float_as_uint(P.rcp[j]));
+    if (warp == 0) tmem_alloc(S.slot, 2 * AS);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *slot;
-    bool ok = mbar_wait_bounded(bar_b, 0);
+    const uint32_t tmem = *S.slot;
+    uint32_t issued = 0;  // tiles whose MMAs thread 0 issued
+    bool b_seen = false;  // thread 0 has seen the B image land
 
-    const uint32_t sbo = 8u * (uint32_t)kb;
-    const uint32_t tlane = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-    uint32_t i = 0;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
-        const uint32_t b = tile / tiles_per_batch;
-        const uint32_t pos0 = (tile - b * tiles_per_batch) * TC_M;
-        const int cnt = (int)min((uint32_t)TC_M, npos - pos0);
-        const bool valid = m < cnt;
-        if (use_bulk) {
-            ok = ok && mbar_wait_bounded(bar_r, i & 1);
-        } else if (gather == CRT_GATHER_VEC) {
-            // runs of 4 positions are 4 consecutive residues (cw, col0 multiples of 4): one
-            // 16-byte load per prime and run, spread over all 256 threads
-            const uint32_t* Rb = R + (size_t)b * K * P.N;
-            for (int idx = threadIdx.x; idx < K * (TC_M / 4); idx += blockDim.x) {
-                const int j = idx / (TC_M / 4), q4 = 4 * (idx % (TC_M / 4));
-                uint4 v = make_uint4(0, 0, 0, 0);
-                if (q4 < cnt) v = *reinterpret_cast<const uint4*>(Rb + (size_t)j * P.N + chunk_pos_to_n(P, C, pos0 + q4));
-                *reinterpret_cast<uint4*>(rt + (size_t)j * TC_M + q4) = v;
-            }
-        } else if (hf == 0) {
-            const uint32_t* Rb = R + (size_t)b * K * P.N;
-            const uint32_t n = valid ? chunk_pos_to_n(P, C, pos0 + m) : 0;
-            for (int j = 0; j < K; ++j) rt[(size_t)j * TC_M + m] = valid ? Rb[(size_t)j * P.N + n] : 0u;
-        }
-        if (__syncthreads_or(!ok)) break;
-
-        // prologue: y_j for 4 primes -> one 16-byte core-matrix row; partial fp32 sums in 4 chains
-        float s4[4] = {0.f, 0.f, 0.f, 0.f};
-        const int g0 = hf ? gh : 0, g1 = hf ? kgroups : gh;
-        for (int g = g0; g < g1; ++g) {
-            uint32_t y[4] = {0, 0, 0, 0};
+    if (threadIdx.x < CRT_PROD_THREADS) {
+        // ---------------- producers ----------------
+        const int m = threadIdx.x & (TC_M - 1), h = threadIdx.x >> 7;
+        const int kgroups = kb / 16;
+        const int gh = (kgroups + 1) / 2;
+        const int g0 = h ? gh : 0, ng = (h ? kgroups : gh) - g0;
+        uint32_t i = 0;
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            if (named_sync_or(1, CRT_PROD_THREADS, *S.abort != 0)) break;
+            const int b = (int)(i & 1);
+            const uint32_t bt = tile / tiles_per_batch;
+            const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
+            const bool valid = (uint32_t)m < npos - pos0;
+            const uint32_t* Rm = R + (size_t)bt * K * P.N + (valid ? chunk_pos_to_n(P, C, pos0 + m) : 0u);
+            uint4 y[CRT_MAX_HALF_GROUPS];
+            float s4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int j = 4 * g + q;
-                if (j < K) {
-                    const uint32_t p = cp[j];
-                    y[q] = red_once(mul_ms(rt[(size_t)j * TC_M + m], cc[j], ccc[j], p), p);
-                    s4[q] = fmaf((float)y[q], crc[j], s4[q]);
+            for (int gg = 0; gg < CRT_MAX_HALF_GROUPS; ++gg) {
+                uint32_t x[4] = {0u, 0u, 0u, 0u};
+                if (gg < ng) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int j = 4 * (g0 + gg) + q;
+                        if (j < K && valid) x[q] = __ldg(Rm + (size_t)j * P.N);
+                    }
+                }
+                uint32_t yy[4] = {0u, 0u, 0u, 0u};
+                if (gg < ng) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int j = 4 * (g0 + gg) + q;
+                        if (j < K) {
+                            const uint4 c = S.cst[j];
+                            yy[q] = red_once(mul_ms(x[q], c.y, c.z, c.x), c.x);
+                            s4[q] = fmaf((float)yy[q], __uint_as_float(c.w), s4[q]);
+                        }
+                    }
+                }
+                y[gg] = make_uint4(yy[0], yy[1], yy[2], yy[3]);
+            }
+            // the previous tile's MMA must have read the A tile; the epilogue of tile i - 2
+            // must have read partial sums [b] (it arrives on acc_empty[b] after that)
+            if (i > 0) wait_or_abort(mma_done + ((i - 1) & 1), ((i - 1) >> 1) & 1, S.abort);
+            if (i > 1) wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
+#pragma unroll
+            for (int gg = 0; gg < CRT_MAX_HALF_GROUPS; ++gg)
+                if (gg < ng)
+                    *reinterpret_cast<uint4*>(S.a + (size_t)(m >> 3) * sbo + (size_t)(g0 + gg) * 128 + (m & 7) * 16) =
+                        y[gg];
+            S.spart[(b * 2 + h) * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            fence_smem_to_async();
+            named_sync(1, CRT_PROD_THREADS);
+            if (threadIdx.x == 0) {
+                bool ok = *S.abort == 0;
+                if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, S.abort);
+                if (ok) {
+                    tc_fence_after();
+                    const uint32_t acc = tmem + (uint32_t)b * AS;
+                    issue_gemm_rows(acc, smem_addr(S.a), smem_addr(S.b), 0, nrows_b, kb);
+                    umma_commit(mma_done + b);
+                    ++issued;
+                }
+                mbar_arrive(v_ready + b);  // releases this tile's partial sums
+            }
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        const int et = threadIdx.x - CRT_PROD_THREADS;
+        const int hf = et >> 7, m = (warp & 3) * 32 + lane;
+        const int nl = nrows_b / 4;                 // limbs covered by the accumulator columns
+        const int lh = ((nl + 1) / 2 + 3) / 4 * 4;  // limbs of half 0 (multiple of 4: 16 columns)
+        uint32_t* z = S.z + (size_t)m * zs;
+        uint32_t i = 0;
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            if (named_sync_or(2, CRT_EPI_THREADS, *S.abort != 0)) break;
+            const int b = (int)(i & 1);
+            const uint32_t bt = tile / tiles_per_batch;
+            const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
+            const int cnt = (int)min((uint32_t)TC_M, npos - pos0);
+            const bool valid = m < cnt;
+            // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
+            const bool got = __all_sync(0xffffffffu, wait_or_abort(v_ready + b, (i >> 1) & 1, S.abort) &&
+                                                         wait_or_abort(mma_done + b, (i >> 1) & 1, S.abort));
+            tc_fence_after();
+            const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
+            const float vf = rintf(sum);
+            if (hf == 0 && valid && got && fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
+            const int v = min(max((int)vf, 0), K);
+            // accumulator bytes -> limbs with carries, + T_v; half hf owns limbs [0, lh) or [lh, zl)
+            const uint32_t* T = P.tneg + (size_t)v * L;
+            const uint32_t tacc = tmem + (uint32_t)b * AS + ((uint32_t)((warp & 3) * 32) << 16);
+            uint64_t carry = 0;
+            const int c0 = hf ? lh / 4 : 0, c1 = hf ? nl / 4 : lh / 4;
+            int l = 4 * c0;
+            for (int c16 = c0; c16 < c1; ++c16) {
+                uint32_t r[16];
+                if (got) tmem_ld16(tacc + (uint32_t)(16 * c16), r);
+                else
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) r[k] = 0u;
+#pragma unroll
+                for (int q = 0; q < 4; ++q, ++l) {
+                    const uint64_t t = carry + (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
+                                       ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24) +
+                                       (l < L ? __ldg(T + l) : 0u);
+                    if (l < zl) z[l] = (uint32_t)t;
+                    carry = t >> 32;
                 }
             }
-            *reinterpret_cast<uint4*>(a_s + (size_t)(m >> 3) * sbo + (size_t)g * 128 + (m & 7) * 16) =
-                make_uint4(y[0], y[1], y[2], y[3]);
-        }
-        spart[hf * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
-        fence_smem_to_async();
-        __syncthreads();
-        const float s = spart[m] + spart[TC_M + m];
-        const float vf = rintf(s);
-        if (hf == 0 && valid && fabsf(s - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
-        const int v = min(max((int)vf, 0), K);
-        if (warp == 0) {
-            const uint32_t nxt = tile + gridDim.x;
-            if (use_bulk && nxt < ntiles) issue_r(nxt);  // rt was consumed before the barrier
-            if (lane == 0) {
-                tc_fence_after();
-                issue_gemm_rows(tmem, smem_addr(a_s), smem_addr(b_s), 0, min(nrows_b, 256), kb);
-                if (nrows_b > 256) issue_gemm_rows(tmem + 256, smem_addr(a_s), smem_addr(b_s), 256, nrows_b - 256, kb);
-                umma_commit(bar_mma);
+            if (hf) {
+                for (; l < zl; ++l) {
+                    z[l] = (uint32_t)carry;
+                    carry >>= 32;
+                }
             }
-            __syncwarp();
-        }
-        const bool got = mbar_wait_bounded(bar_mma, i & 1);
-        if (__syncthreads_or(!got)) {
-            ok = false;
-            break;
-        }
-        tc_fence_after();
-
-        // epilogue: accumulator bytes -> limbs with carries, + T_v; half h owns limbs
-        // [0, lh) or [lh, zl) of this coefficient's staging row
-        uint32_t* z = z_s + (size_t)m * zs;
-        const uint32_t* T = P.tneg + (size_t)v * L;
-        uint64_t carry = 0;
-        const int c0 = hf ? lh / 4 : 0, c1 = hf ? nl / 4 : lh / 4;
-        int l = 4 * c0;
-        for (int c16 = c0; c16 < c1; ++c16) {
-            uint32_t r[16];
-            tmem_ld16(tlane + (uint32_t)(16 * c16), r);
+            tc_fence_before();
+            mbar_arrive(acc_empty + b);  // accumulator b and partial sums b are free again
+            named_sync(2, CRT_EPI_THREADS);
+            if (hf == 0 && valid) {
+                for (int k = lh; carry && k < zl; ++k) {  // half 0's carry-out into half 1's limbs
+                    const uint64_t t = (uint64_t)z[k] + carry;
+                    z[k] = (uint32_t)t;
+                    carry = t >> 32;
+                }
+                crt_reduce_mod_q(z, zl, P);
+            }
+            named_sync(2, CRT_EPI_THREADS);
+            // coalesced store of the tile's cnt x L limbs (contiguous in the output)
+            uint32_t* o = out + ((size_t)bt * npos + pos0) * L;
+            const int tot = cnt * L;
+            int w = et;
+            for (; w + 3 * CRT_EPI_THREADS < tot; w += 4 * CRT_EPI_THREADS) {
+                uint32_t v4[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q, ++l) {
-                const uint64_t t = carry + (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
-                                   ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24) +
-                                   (l < L ? __ldg(T + l) : 0u);
-                if (l < zl) z[l] = (uint32_t)t;
-                carry = t >> 32;
+                for (int u = 0; u < 4; ++u) {
+                    const int ww = w + u * CRT_EPI_THREADS, mm = ww / L;
+                    v4[u] = S.z[(size_t)mm * zs + (ww - mm * L)];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) o[w + u * CRT_EPI_THREADS] = v4[u];
+            }
+            for (; w < tot; w += CRT_EPI_THREADS) {
+                const int mm = w / L;
+                o[w] = S.z[(size_t)mm * zs + (w - mm * L)];
             }
         }
-        if (hf) {
-            for (; l < zl; ++l) {
-                z[l] = (uint32_t)carry;
-                carry >>= 32;
-            }
-        }
-        __syncthreads();
-        if (hf == 0 && valid) {
-            for (int k = lh; carry && k < zl; ++k) {  // half 0's carry-out into half 1's limbs
-                const uint64_t t = (uint64_t)z[k] + carry;
-                z[k] = (uint32_t)t;
-                carry = t >> 32;
-            }
-            crt_reduce_mod_q(z, zl, P);
-        }
-        __syncthreads();
-        uint32_t* o = out + ((size_t)b * npos + pos0) * L;
-        for (int mm = warp; mm < cnt; mm += 8)
-            for (int ll = lane; ll < L; ll += 32) o[(size_t)mm * L + ll] = z_s[(size_t)mm * zs + ll];
-        tc_fence_before();
-        __syncthreads();
     }
-    if (!ok && threadIdx.x == 0) flag_error(P.status, DEV_ERR_WAIT);
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, ncols);
+    if (threadIdx.x == 0 && *S.abort) {
+        flag_error(P.status, DEV_ERR_WAIT);
+        // copies and MMAs still in flight must land before this CTA's memory goes away
+        if (!b_seen) mbar_wait_bounded(bar_b, 0);
+        if (issued) mbar_wait_bounded(mma_done + ((issued - 1) & 1), ((issued - 1) >> 1) & 1);
+    }
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 2 * AS);
 }
 
 size_t rns_tc_smem(const DevPlan& P) {
@@ -478,8 +570,8 @@ size_t rns_tc_smem(const DevPlan& P) {
 }
 
 size_t crt_tc_smem(const DevPlan& P) {
-    return (size_t)P.crt_nrows * P.crt_kbytes + crt_a_bytes(P) + (size_t)P.K * TC_M * 4 + (size_t)P.KP * 16 +
-           2 * TC_M * 4 + 64;
+    return (size_t)P.crt_nrows * P.crt_kbytes + (size_t)TC_M * P.crt_kbytes + crt_z_bytes(P) + (size_t)P.KP * 16 +
+           4 * TC_M * 4 + 7 * 8 + 16;
 }
 
 }  // namespace pm

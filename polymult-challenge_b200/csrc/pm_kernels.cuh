@@ -40,14 +40,9 @@ size_t crt_plain_smem(const DevPlan& P);
 constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
 __global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R,
                          int use_bulk);
-__global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
-                         int gather);
-// how k_crt_tc gathers a tile's residues: per-prime bulk copies of whole 128-byte row
-// segments (chunks >= 32 columns), 16-byte loads by every thread (narrower chunks of a
-// multiple of 4 columns), or 4-byte loads
-enum : int { CRT_GATHER_SCALAR = 0, CRT_GATHER_VEC = 1, CRT_GATHER_BULK = 2 };
+__global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out);
 constexpr int RNS_TC_THREADS = 256;  // 8 epilogue warps: 4 TMEM lane quarters x 2 prime halves
-constexpr int CRT_TC_THREADS = 256;  // two threads per coefficient / TMEM lane
+constexpr int CRT_TC_THREADS = 512;  // 256 producers + 256 epilogue threads, two per coefficient each
 size_t rns_tc_smem(const DevPlan& P);
 size_t crt_tc_smem(const DevPlan& P);
 // TMEM columns to allocate: a power of two >= max(32, n)
@@ -68,10 +63,6 @@ __host__ __device__ inline uint32_t dec_half1_col(int n0) { return (uint32_t)((n
 // words of one CRT staging row: z needs L + 3 limbs (value < 2^(W + 64)); odd stride
 __host__ __device__ inline int crt_zl(int L) { return L + 3; }
 __host__ __device__ inline int crt_zstride(int L) { return crt_zl(L) | 1; }
-// bytes of the CRT A tile region (also holds the z staging rows after the MMA)
-__host__ __device__ inline size_t crt_a_bytes(const DevPlan& P) {
-    const size_t a = (size_t)TC_M * P.crt_kbytes, z = (size_t)TC_M * crt_zstride(P.L) * 4;
-    return a > z ? a : z;
-}
+
 
 }  // namespace pm
