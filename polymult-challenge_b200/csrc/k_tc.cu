@@ -150,10 +150,13 @@ __device__ __forceinline__ void bulk_g2s_all(void* dst, const void* src, uint32_
 // Per tile: the raw coefficients (contiguous cnt*L words) arrive by one bulk copy into a
 // double-buffered ring, prefetched two tiles ahead; all warps re-lay them out as the K-major
 // A operand; thread 0 issues the MMAs of the two prime halves with one commit each, so the
-// epilogue of half 0 overlaps the MMA of half 1.
+// epilogue of half 0 overlaps the MMA of half 1.  512 threads: warp w reads TMEM lane quarter
+// w % 4 of prime half (w / 4) % 2, and of that half's 16-column chunks those with index
+// parity w / 8 -- four warps per lane quarter, so that the REDC epilogue (the longest phase)
+// has 16 warps to hide its latencies.
 // smem: [B image][A tile][raw ring 2 x 128*L words][bars: B, raw0, raw1, mma0, mma1][slot]
 // ----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 1) k_rns_tc(DevPlan P, const uint32_t* __restrict__ src, ChunkMap C,
+__global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const uint32_t* __restrict__ src, ChunkMap C,
                                                    uint32_t npos, uint32_t nbatch, uint32_t* __restrict__ R,
                                                    int use_bulk) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -202,7 +205,7 @@ __global__ void __launch_bounds__(256, 1) k_rns_tc(DevPlan P, const uint32_t* __
 
     const uint32_t sbo = 8u * (uint32_t)kb;
     const int groups = kb / 16;
-    const int half = warp >> 2, m = (warp & 3) * 32 + lane;
+    const int half = (warp >> 2) & 1, sub = warp >> 3, m = (warp & 3) * 32 + lane;
     uint32_t i = 0;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
         const int buf = (int)(i & 1);
@@ -247,7 +250,8 @@ __global__ void __launch_bounds__(256, 1) k_rns_tc(DevPlan P, const uint32_t* __
             }
         }
         if (half == 0 || n1 > 0) {
-            const bool got = mbar_wait_bounded(bar_mma + half, i & 1);
+            // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
+            const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(bar_mma + half, i & 1));
             if (!got) flag_error(P.status, DEV_ERR_WAIT);
             tc_fence_after();
             const uint32_t b = tile / tiles_per_batch;
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(256, 1) k_rns_tc(DevPlan P, const uint32_t* __
             const int j0 = half ? KH : 0;
             const int cols = half ? n1 : n0;
             const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
-            for (int c16 = 0; c16 < cols / 16 && got; ++c16) {
+            for (int c16 = sub; c16 < cols / 16 && got; c16 += 2) {
                 uint32_t r[16];
                 tmem_ld16(tcol + (uint32_t)(16 * c16), r);
 #pragma unroll
@@ -307,7 +311,7 @@ namespace {
 
 constexpr int CRT_PROD_THREADS = 256;
 constexpr int CRT_EPI_THREADS = 256;
-constexpr int CRT_MAX_HALF_GROUPS = 16;  // KP <= 128: 4 KP / 16 <= 32 groups of 4 primes, 16 per half
+constexpr int CRT_BATCH_GROUPS = 3;      // prime groups (4 primes each) per batch of producer loads
 
 __device__ __forceinline__ void named_sync(int id, int n) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
@@ -421,41 +425,52 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
             const bool valid = (uint32_t)m < npos - pos0;
             const uint32_t* Rm = R + (size_t)bt * K * P.N + (valid ? chunk_pos_to_n(P, C, pos0 + m) : 0u);
-            uint4 y[CRT_MAX_HALF_GROUPS];
+            // residues in batches of CRT_BATCH_GROUPS groups (4 primes each), the next batch's
+            // loads in flight while this batch is converted: up to 2 x 16 loads per thread
             float s4[4] = {0.f, 0.f, 0.f, 0.f};
+            uint32_t xa[4 * CRT_BATCH_GROUPS], xb[4 * CRT_BATCH_GROUPS];
+            auto load_batch = [&](uint32_t(&x)[4 * CRT_BATCH_GROUPS], int bat) {
 #pragma unroll
-            for (int gg = 0; gg < CRT_MAX_HALF_GROUPS; ++gg) {
-                uint32_t x[4] = {0u, 0u, 0u, 0u};
-                if (gg < ng) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int j = 4 * (g0 + gg) + q;
-                        if (j < K && valid) x[q] = __ldg(Rm + (size_t)j * P.N);
-                    }
+                for (int u = 0; u < 4 * CRT_BATCH_GROUPS; ++u) {
+                    const int gg = bat * CRT_BATCH_GROUPS + u / 4, j = 4 * (g0 + gg) + (u & 3);
+                    x[u] = (gg < ng && j < K && valid) ? __ldg(Rm + (size_t)j * P.N) : 0u;
                 }
-                uint32_t yy[4] = {0u, 0u, 0u, 0u};
-                if (gg < ng) {
+            };
+            auto convert_batch = [&](const uint32_t(&x)[4 * CRT_BATCH_GROUPS], int bat) {
+#pragma unroll
+                for (int gl = 0; gl < CRT_BATCH_GROUPS; ++gl) {
+                    const int gg = bat * CRT_BATCH_GROUPS + gl;
+                    if (gg >= ng) break;
+                    uint32_t yy[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int j = 4 * (g0 + gg) + q;
+                        yy[q] = 0u;
                         if (j < K) {
                             const uint4 c = S.cst[j];
-                            yy[q] = red_once(mul_ms(x[q], c.y, c.z, c.x), c.x);
+                            yy[q] = red_once(mul_ms(x[4 * gl + q], c.y, c.z, c.x), c.x);
                             s4[q] = fmaf((float)yy[q], __uint_as_float(c.w), s4[q]);
                         }
                     }
-                }
-                y[gg] = make_uint4(yy[0], yy[1], yy[2], yy[3]);
-            }
-            // the previous tile's MMA must have read the A tile; the epilogue of tile i - 2
-            // must have read partial sums [b] (it arrives on acc_empty[b] after that)
-            if (i > 0) wait_or_abort(mma_done + ((i - 1) & 1), ((i - 1) >> 1) & 1, S.abort);
-            if (i > 1) wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
-#pragma unroll
-            for (int gg = 0; gg < CRT_MAX_HALF_GROUPS; ++gg)
-                if (gg < ng)
                     *reinterpret_cast<uint4*>(S.a + (size_t)(m >> 3) * sbo + (size_t)(g0 + gg) * 128 + (m & 7) * 16) =
-                        y[gg];
+                        make_uint4(yy[0], yy[1], yy[2], yy[3]);
+                }
+            };
+            const int nbat = (ng + CRT_BATCH_GROUPS - 1) / CRT_BATCH_GROUPS;
+            load_batch(xa, 0);
+            // the previous tile's MMA must have read the A tile before it is overwritten
+            if (i > 0) wait_or_abort(mma_done + ((i - 1) & 1), ((i - 1) >> 1) & 1, S.abort);
+            for (int bat = 0; bat < nbat; bat += 2) {
+                if (bat + 1 < nbat) load_batch(xb, bat + 1);
+                convert_batch(xa, bat);
+                if (bat + 1 < nbat) {
+                    if (bat + 2 < nbat) load_batch(xa, bat + 2);
+                    convert_batch(xb, bat + 1);
+                }
+            }
+            // the epilogue of tile i - 2 must have read partial sums [b] (it arrives on
+            // acc_empty[b] after that)
+            if (i > 1) wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
             S.spart[(b * 2 + h) * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
             fence_smem_to_async();
             named_sync(1, CRT_PROD_THREADS);
@@ -495,8 +510,10 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             const float vf = rintf(sum);
             if (hf == 0 && valid && got && fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
             const int v = min(max((int)vf, 0), K);
-            // accumulator bytes -> limbs with carries, + T_v; half hf owns limbs [0, lh) or [lh, zl)
-            const uint32_t* T = P.tneg + (size_t)v * L;
+            // accumulator bytes -> limbs with carries, + v T_1 (T_1 = (-M) mod q; v T_1 == T_v mod q,
+            // < 2^(W+7), and the fold below reduces it; one row for every lane instead of a
+            // per-lane row T_v); half hf owns limbs [0, lh) or [lh, zl)
+            const uint32_t* T1 = P.tneg + L;
             const uint32_t tacc = tmem + (uint32_t)b * AS + ((uint32_t)((warp & 3) * 32) << 16);
             uint64_t carry = 0;
             const int c0 = hf ? lh / 4 : 0, c1 = hf ? nl / 4 : lh / 4;
@@ -511,7 +528,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 for (int q = 0; q < 4; ++q, ++l) {
                     const uint64_t t = carry + (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
                                        ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24) +
-                                       (l < L ? __ldg(T + l) : 0u);
+                                       (l < L ? (uint64_t)(uint32_t)v * __ldg(T1 + l) : 0ull);
                     if (l < zl) z[l] = (uint32_t)t;
                     carry = t >> 32;
                 }

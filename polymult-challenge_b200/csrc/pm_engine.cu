@@ -376,10 +376,12 @@ void Engine::setup_host_pipeline() {
     mk(ev_out_, cout_.size());
     cuda_check(cudaEventCreateWithFlags(&ev_row_a_, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
-    // 12 copying threads (11 workers + the caller) when the host has 14 or more CPUs: on the
-    // B200 hosts measured, 12 threads finish staging a 28.8 MB operand pair in 0.63 ms against
-    // 1.0 ms for 8; POLYMULT_HOST_THREADS overrides
-    int workers = std::max(0, std::min(11, usable_cpus() - 3));
+    // 8 copying threads (7 workers + the caller) by default.  On the 16-CPU B200 hosts measured,
+    // 12 threads stage an operand pair faster in isolation (0.63 ms against 1.0 ms) but made the
+    // end-to-end call slower and far more variable inside a full process (p50 1.51 ms, p99 5.6 ms
+    // against 1.13 / 1.2 ms): spinning workers then compete with the process's other threads.
+    // POLYMULT_HOST_THREADS overrides.
+    int workers = std::max(0, std::min(7, usable_cpus() - 2));
     if (const char* e = std::getenv("POLYMULT_HOST_THREADS")) workers = std::max(0, std::min(63, std::atoi(e) - 1));
     pool_.reset(new HostPool(workers));
 }
