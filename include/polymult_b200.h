@@ -53,7 +53,7 @@ typedef struct pm_info {
     uint64_t table_bytes;  /* device memory of the per-point tables */
     uint64_t scratch_bytes;/* device memory of the residue scratch */
     int32_t launches_per_multiply; /* kernels launched per device-resident multiply group */
-    int32_t group;         /* multiplies per launch group of pm_run_device (scratch sized for it) */
+    int32_t group;         /* multiplies per launch group of pm_run_device (its scratch grows to this on use) */
 } pm_info;
 
 /* Replaces fherma_init (solve.cu:1392-1478): validates the point, builds every table,
@@ -190,6 +190,21 @@ int pm_server_run(pm_server* server, uint32_t n, const double* t_arrive, const u
 int pm_server_host_alloc(pm_server* server, size_t bytes, void** out);
 int pm_server_host_free(pm_server* server, void* p);
 void pm_server_free(pm_server* server);
+
+/* The host pipeline's column-chunk schedule.  The reference fixes it (make_chunks,
+ * solve.cu:1085-1108, with the divisors of solve.cu:1403-1405). */
+typedef struct pm_pipeline_info {
+    int32_t in_chunks, out_chunks;  /* column chunks per input operand / of the output */
+    int32_t in_body, out_body;      /* body chunk = ncols / divisor */
+    double tuned_ms;                /* median pm_run time of the chosen schedule (0: not tuned) */
+} pm_pipeline_info;
+
+/* No reference counterpart: the autotuner of the host pipeline.  Runs `reps` pm_run calls (plus
+ * a warm-up) for every schedule with body divisors in {4, 8, 16} x {4, 8, 16}, keeps the one
+ * with the lowest median wall time, and describes it in *out.  Synchronous; about 10 x (reps + 1)
+ * calls. */
+int pm_tune_pipeline(pm_context* ctx, int reps, pm_pipeline_info* out);
+int pm_get_pipeline(const pm_context* ctx, pm_pipeline_info* out);
 
 /* Waits for the context's device work and returns PM_ERR_DEVICE if a device-side check
  * failed since the last call. */

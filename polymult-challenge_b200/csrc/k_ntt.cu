@@ -94,10 +94,11 @@ struct RowCfg : LineCfg<NB> {
              : NB == 10          ? (i == 0 ? 1u : i == 1 ? 18u : i == 2 ? 4u : i == 3 ? 8u : 0u)
                                  : 0u;
     }
-    static __device__ __forceinline__ int swz(int X) {
-        const int h = X >> 5;
-        return X ^ ((h & 1 ? (int)g(0) : 0) ^ (h & 2 ? (int)g(1) : 0) ^ (h & 4 ? (int)g(2) : 0) ^
-                    (h & 8 ? (int)g(3) : 0) ^ (h & 16 ? (int)g(4) : 0));
+    // X ^ G(X >> 5) is linear over XOR: swz(a ^ b) = swz(a) ^ swz(b), so an element's address
+    // is the thread's swizzled base XOR a compile-time constant
+    __host__ __device__ static constexpr int swz(int X) {
+        return X ^ (((X >> 5) & 1 ? (int)g(0) : 0) ^ ((X >> 5) & 2 ? (int)g(1) : 0) ^ ((X >> 5) & 4 ? (int)g(2) : 0) ^
+                    ((X >> 5) & 8 ? (int)g(3) : 0) ^ ((X >> 5) & 16 ? (int)g(4) : 0));
     }
 };
 
@@ -119,11 +120,13 @@ __device__ __forceinline__ int row_x(int r, int e) {
 template <int NB, int K, bool TO_SMEM>
 __device__ __forceinline__ void row_xchg(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r) {
     using C = RowCfg<NB>;
-    if constexpr (C::VEC && C::b0(K) == 0) {
-        const int X0 = (rho << NB) | row_x<NB, K>(r, 0);
+    constexpr int b0 = C::b0(K);
+    // the register bits of X are zero in the base: X(e) = base ^ (e << b0)
+    const int sbase = C::swz((rho << NB) | row_x<NB, K>(r, 0));
+    if constexpr (C::VEC && b0 == 0) {
 #pragma unroll
         for (int q = 0; q < C::E / 4; ++q) {
-            uint4* a = reinterpret_cast<uint4*>(region + C::swz(X0 + 4 * q));
+            uint4* a = reinterpret_cast<uint4*>(region + (sbase ^ C::swz(4 * q)));
             if (TO_SMEM) *a = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             else {
                 const uint4 u = *a;
@@ -136,7 +139,7 @@ __device__ __forceinline__ void row_xchg(uint32_t (&v)[RowCfg<NB>::E], uint32_t*
     } else {
 #pragma unroll
         for (int e = 0; e < C::E; ++e) {
-            uint32_t* a = region + C::swz((rho << NB) | row_x<NB, K>(r, e));
+            uint32_t* a = region + (sbase ^ C::swz(e << b0));
             if (TO_SMEM) *a = v[e];
             else v[e] = *a;
         }
@@ -185,6 +188,7 @@ __device__ __forceinline__ void row_forward(uint32_t (&v)[RowCfg<NB>::E], uint32
     if constexpr (K < C::NPH) {
         constexpr int b0 = C::b0(K);
         const uint32_t hip = (uint32_t)(r >> b0);  // index bits above the registers
+        // per local stage t: the row's run of twiddles, tw[2^(w1+ls) + hi 2^ls + (hip << t) + m]
         auto tw = [&](int t, int m) {
             const int ls = C::ls(K, t);
             return make_tw(__ldg(twj + (1u << (w1 + ls)) + (hi << ls) + ((hip << t) | (uint32_t)m)), pinv);
@@ -210,6 +214,7 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
     if constexpr (K >= 0) {
         constexpr int b0 = C::b0(K);
         const uint32_t hip = (uint32_t)(r >> b0);
+        // tw[2^(w1+ls) + hi_m 2^ls + 2^ls - 1 - ((hip << t) + m)]
         auto tw = [&](int t, int m) {
             const int ls = C::ls(K, t);
             const uint32_t gi = (hip << t) | (uint32_t)m;
@@ -297,24 +302,29 @@ __device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32
     for (int gidx = threadIdx.x >> ltc; gidx < NGRP; gidx += slots) {
         const int lo = gidx & ((1 << b0) - 1), hip = gidx >> b0;
         const int xb = (hip << (b0 + C::RB)) | lo;
+        // element e is row xb + (e << b0): global offset gb + e (gstride << b0), tile offset sb + e (tc << b0)
+        uint32_t* gb = gbase + (size_t)xb * gstride + c;
+        uint32_t* sb = tile + (xb << ltc) + c;
+        const size_t gstep = gstride << b0;
+        const int sstep = 1 << (b0 + ltc);
         uint32_t v[C::E];
 #pragma unroll
-        for (int e = 0; e < C::E; ++e) {
-            const int x = xb | (e << b0);
-            v[e] = FIRST ? gbase[(size_t)x * gstride + c] : tile[(x << ltc) + c];
-        }
+        for (int e = 0; e < C::E; ++e) v[e] = FIRST ? gb[e * gstep] : sb[e * sstep];
+        int tb[C::RB];
+#pragma unroll
+        for (int t = 0; t < C::RB; ++t)
+            tb[t] = INV ? (2 << C::ls(K, t)) - 1 - (hip << t) : (1 << C::ls(K, t)) + (hip << t);
         if (!INV) {
-            auto tw = [&](int t, int m) { return tws[(1 << C::ls(K, t)) + ((hip << t) | m)]; };
+            auto tw = [&](int t, int m) { return tws[tb[t] + m]; };
             radix_fwd<C::RB, C::t0(K)>(v, tw, p);
         } else {
-            auto tw = [&](int t, int m) { return tws[(2 << C::ls(K, t)) - 1 - ((hip << t) | m)]; };
+            auto tw = [&](int t, int m) { return tws[tb[t] - m]; };
             radix_inv<C::RB, C::t0(K)>(v, tw, p);
         }
 #pragma unroll
         for (int e = 0; e < C::E; ++e) {
-            const int x = xb | (e << b0);
-            if (LAST) gbase[(size_t)x * gstride + c] = v[e];
-            else tile[(x << ltc) + c] = v[e];
+            if (LAST) gb[e * gstep] = v[e];
+            else sb[e * sstep] = v[e];
         }
     }
 }

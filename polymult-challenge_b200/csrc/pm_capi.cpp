@@ -123,6 +123,30 @@ int pm_get_info(const pm_context* ctx, pm_info* out) {
     return PM_OK;
 }
 
+static void fill_pipeline(const pm::Engine& e, double ms, pm_pipeline_info* out) {
+    std::memset(out, 0, sizeof *out);
+    out->in_chunks = (int32_t)e.in_chunks().size();
+    out->out_chunks = (int32_t)e.out_chunks().size();
+    out->in_body = (int32_t)e.in_body();
+    out->out_body = (int32_t)e.out_body();
+    out->tuned_ms = ms;
+}
+
+int pm_tune_pipeline(pm_context* ctx, int reps, pm_pipeline_info* out) {
+    if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    return guarded([&] {
+        const double ms = ctx->engine->tune_host_pipeline(reps);
+        ctx->tuned_ms = ms;
+        if (out) fill_pipeline(*ctx->engine, ms, out);
+    });
+}
+
+int pm_get_pipeline(const pm_context* ctx, pm_pipeline_info* out) {
+    if (!ctx || !ctx->engine || !out) return fail(PM_ERR_INVALID, "null argument");
+    fill_pipeline(*ctx->engine, ctx->tuned_ms, out);
+    return PM_OK;
+}
+
 int pm_batch_init(const pm_batch_class* classes, uint32_t nclasses, int gemm_form, int flags, int device,
                   pm_batch** out) {
     if (!out) return fail(PM_ERR_INVALID, "out is null");

@@ -227,9 +227,15 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
             smem_dec_ = rns_tc_smem(dp_);
             smem_crt_ = crt_tc_smem(dp_);
         }
-        // one multiply's worth of residues per group at the ranked size; more for small N
+        // multiplies per launch group of run_device: up to POLYMULT_GROUP_WORDS residue words
+        // per operand (default 64 Mi: 8 multiplies at N = 65536, W = 1747, 512 MB of residue
+        // scratch), at most 256.  Measured there: 1 multiply per group 4083 mults/s, 2 4789,
+        // 8 5144 -- every kernel's fixed costs (B image, ramp, last partial wave) amortise over
+        // the group, which outweighs keeping one multiply's residues in L2.
+        size_t group_words = size_t(64) << 20;
+        if (const char* e = std::getenv("POLYMULT_GROUP_WORDS")) group_words = std::max<size_t>(1, std::strtoull(e, nullptr, 10));
         const size_t per_mult = (size_t)plan_.K * plan_.N;
-        group_cap_ = (uint32_t)std::max<size_t>(1, std::min<size_t>(256, (8u << 20) / std::max<size_t>(1, per_mult)));
+        group_cap_ = (uint32_t)std::max<size_t>(1, std::min<size_t>(256, group_words / std::max<size_t>(1, per_mult)));
         if (opt.host_pipeline) {
             ensure_scratch(1);
             setup_host_pipeline();
@@ -345,10 +351,64 @@ void Engine::ensure_scratch(uint32_t group) {
     group_ = group;
 }
 
-void Engine::setup_host_pipeline() {
+// Column-chunk schedule of the host pipeline: input chunks of ncols / in_body columns after
+// narrow head chunks (1/32, 1/32, 1/16), output chunks of ncols / out_body columns between
+// narrow head and tail chunks (1/64, 1/32 ... 1/32, 1/64), so that the pipeline fills and
+// drains sooner; events sized to match.
+void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body) {
+    if (in_body == 0 || out_body == 0 || (in_body & (in_body - 1)) || (out_body & (out_body - 1)))
+        throw InvalidPoint("chunk divisors must be powers of two");
     const uint32_t nc = plan_.ncols;
-    cin_ = make_chunks(nc, {32, 32, 16}, 8, {});
-    cout_ = make_chunks(nc, {64, 32}, 8, {32, 64});
+    cin_ = make_chunks(nc, {32, 32, 16}, in_body, {});
+    cout_ = make_chunks(nc, {64, 32}, out_body, {32, 64});
+    in_body_ = in_body;
+    out_body_ = out_body;
+    auto mk = [](std::vector<cudaEvent_t>& v, size_t n, unsigned flags) {
+        for (auto e : v) cudaEventDestroy(e);
+        v.assign(n, nullptr);
+        for (auto& e : v) cuda_check(cudaEventCreateWithFlags(&e, flags), "event");
+    };
+    mk(ev_in_, 2 * cin_.size(), cudaEventDisableTiming);
+    mk(ev_done_in_, 2 * cin_.size(), cudaEventDisableTiming);
+    mk(ev_crt_, cout_.size(), cudaEventDisableTiming);
+    mk(ev_out_, cout_.size(), cudaEventDisableTiming);
+    if (profile_) mk(trace_ev_, 8 + 2 * 2 * cin_.size() + 2 * cout_.size(), cudaEventDefault);
+}
+
+// Times every (in_body, out_body) in {4, 8, 16}^2 on `reps` calls of run_host (after one
+// warm-up call each) and keeps the schedule with the lowest median; returns that median (ms).
+double Engine::tune_host_pipeline(int reps) {
+    if (!pool_) throw Unsupported("this context has no host pipeline");
+    reps = std::max(1, reps);
+    std::vector<uint32_t> a(plan_.coeff_words(), 0), c(plan_.coeff_words());
+    for (size_t i = 0; i < a.size(); ++i) a[i] = (uint32_t)(i * 2654435761u) >> 8;  // any in-range limbs
+    double best = 1e30;
+    uint32_t bi = in_body_, bo = out_body_;
+    const uint32_t cand[3] = {4, 8, 16};
+    for (uint32_t ib : cand)
+        for (uint32_t ob : cand) {
+            if (ib > plan_.ncols || ob > plan_.ncols) continue;
+            set_chunk_schedule(ib, ob);
+            run_host(a.data(), a.data(), c.data());
+            std::vector<double> t;
+            for (int r = 0; r < reps; ++r) {
+                const auto t0 = std::chrono::steady_clock::now();
+                run_host(a.data(), a.data(), c.data());
+                t.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+            }
+            std::sort(t.begin(), t.end());
+            const double med = t[t.size() / 2];
+            if (med < best) {
+                best = med;
+                bi = ib;
+                bo = ob;
+            }
+        }
+    set_chunk_schedule(bi, bo);
+    return best;
+}
+
+void Engine::setup_host_pipeline() {
     const size_t bytes = plan_.coeff_words() * 4;
     for (int i = 0; i < 2; ++i) {
         d_in_[i] = dev_alloc<uint32_t>(dev_allocs_, plan_.coeff_words(), nullptr);
@@ -359,21 +419,10 @@ void Engine::setup_host_pipeline() {
     cuda_check(cudaHostAlloc(&h_status_, 16, cudaHostAllocDefault), "cudaHostAlloc");
     *h_status_ = 0;
     profile_ = std::getenv("POLYMULT_PROFILE") != nullptr;
-    if (profile_) {
-        trace_ev_.resize(8 + 2 * 2 * cin_.size() + 2 * cout_.size());
-        for (auto& e : trace_ev_) cuda_check(cudaEventCreate(&e), "event");
-    }
     for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
-    auto mk = [](std::vector<cudaEvent_t>& v, size_t n) {
-        v.resize(n);
-        for (auto& e : v) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-    };
-    mk(ev_in_, 2 * cin_.size());
-    mk(ev_done_in_, 2 * cin_.size());
-    mk(ev_crt_, cout_.size());
-    mk(ev_out_, cout_.size());
+    set_chunk_schedule(8, 8);
     cuda_check(cudaEventCreateWithFlags(&ev_row_a_, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
     // 8 copying threads (7 workers + the caller) by default.  On the 16-CPU B200 hosts measured,

@@ -98,6 +98,12 @@ class Engine {
                      float* ms_out);
     // One multiply from host (pageable) operands to a host result; synchronous.
     void run_host(const uint32_t* a, const uint32_t* b, uint32_t* c);
+    // Host pipeline column-chunk schedule (powers of two: body chunks of ncols / divisor).
+    void set_chunk_schedule(uint32_t in_body, uint32_t out_body);
+    // Measures the candidate schedules on run_host and keeps the fastest; median ms.
+    double tune_host_pipeline(int reps);
+    uint32_t in_body() const { return in_body_; }
+    uint32_t out_body() const { return out_body_; }
     // Reads (and clears) the device status word; synchronises with the device.
     uint32_t take_status();
     void throw_if_status();
@@ -108,7 +114,7 @@ class Engine {
     int device() const { return device_; }
     size_t scratch_bytes() const { return scratch_words_ * 4; }
     size_t table_bytes() const { return table_bytes_; }
-    uint32_t group() const { return group_; }
+    uint32_t group() const { return group_cap_; }  // multiplies per launch group of run_device
     int kernel_launches_per_group() const;
     const std::vector<Chunk>& in_chunks() const { return cin_; }
     const std::vector<Chunk>& out_chunks() const { return cout_; }
@@ -151,6 +157,7 @@ class Engine {
 
     // host pipeline
     std::vector<Chunk> cin_, cout_;
+    uint32_t in_body_ = 8, out_body_ = 8;
     uint32_t* d_in_[2] = {nullptr, nullptr};
     uint32_t* d_out_ = nullptr;
     uint32_t* h_in_[2] = {nullptr, nullptr};

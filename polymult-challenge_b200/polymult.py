@@ -47,6 +47,11 @@ class PmInfo(ctypes.Structure):
                 ("group", ctypes.c_int32)]
 
 
+class PmPipelineInfo(ctypes.Structure):
+    _fields_ = [("in_chunks", ctypes.c_int32), ("out_chunks", ctypes.c_int32), ("in_body", ctypes.c_int32),
+                ("out_body", ctypes.c_int32), ("tuned_ms", ctypes.c_double)]
+
+
 class PmBatchClass(ctypes.Structure):
     _fields_ = [("N", ctypes.c_uint32), ("W", ctypes.c_uint32), ("L", ctypes.c_uint32),
                 ("q", ctypes.c_void_p), ("count", ctypes.c_uint32), ("d_a", ctypes.c_void_p),
@@ -114,6 +119,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_plan_selfcheck.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp,
                                       ctypes.POINTER(ctypes.c_int32)]
     lib.pm_plan_selfcheck.restype = ctypes.c_int
+    lib.pm_tune_pipeline.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
+    lib.pm_tune_pipeline.restype = ctypes.c_int
+    lib.pm_get_pipeline.argtypes = [vp, ctypes.POINTER(PmPipelineInfo)]
+    lib.pm_get_pipeline.restype = ctypes.c_int
     lib.pm_batch_init.argtypes = [ctypes.POINTER(PmBatchClass), ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.POINTER(vp)]
     lib.pm_batch_init.restype = ctypes.c_int
@@ -210,6 +219,17 @@ class Multiplier:
 
     def sync(self):
         _check(load().pm_sync(self._h))
+
+    def tune_pipeline(self, reps: int = 5) -> dict:
+        """Chooses the host pipeline's chunk schedule by measurement (pm_tune_pipeline)."""
+        inf = PmPipelineInfo()
+        _check(load().pm_tune_pipeline(self._h, reps, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in PmPipelineInfo._fields_}
+
+    def pipeline(self) -> dict:
+        inf = PmPipelineInfo()
+        _check(load().pm_get_pipeline(self._h, ctypes.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in PmPipelineInfo._fields_}
 
     def close(self):
         if getattr(self, "_h", None):

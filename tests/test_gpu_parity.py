@@ -140,3 +140,19 @@ def test_fherma_python_mirror():
             polymult.fherma_run(st, a[:-1], b[:-1])
     finally:
         polymult.fherma_free(st)
+
+
+def test_tuned_pipeline_still_bit_exact():
+    """The host pipeline's autotuner (pm_tune_pipeline) only changes the column-chunk schedule:
+    results stay byte-identical to the reference's and the schedule is one of the candidates."""
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (32768, 868))
+    with _multiplier(pt, "tensor") as m:
+        before = m.pipeline()
+        assert before["in_body"] == 8 and before["out_body"] == 8 and before["tuned_ms"] == 0
+        info = m.tune_pipeline(2)
+        assert info["in_body"] in (4, 8, 16) and info["out_body"] in (4, 8, 16) and info["tuned_ms"] > 0
+        assert m.pipeline() == info
+        for case in pt["cases"]:
+            a, b, _ = regen_case(pt, case)
+            assert sha(m.multiply(a, b)) == case["c_sha256"], (case["s"], case["mode"])
+        m.sync()
