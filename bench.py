@@ -381,6 +381,8 @@ def run_batched(torch, args, local):
                 "graph_nodes": inf["graph_nodes"], "kernel_launches": inf["kernel_launches"],
                 "streams": inf["streams"], "scratch_gb": round(inf["scratch_bytes"] / 1e9, 3),
                 "gemm_forms_chosen": forms, "splits_chosen": sorted({(c["w1"], c["w2"]) for c in chosen}),
+                "class_ms": [[k["N"], k["W"], k["count"], c["gemm"], round(c["tuned_ms"], 3)]
+                             for k, c in zip(ks, chosen)],
                 "matches_sequential_plain": same, "tune_cache": tune_cache or "default"})
     return out
 

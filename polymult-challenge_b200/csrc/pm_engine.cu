@@ -119,11 +119,13 @@ int usable_cpus() {
     return (int)std::max(1u, std::thread::hardware_concurrency());
 }
 
-// pageable <-> pinned copy with non-temporal stores where aligned (the destination is not
-// read back by this thread, so skipping its read-for-ownership saves host bandwidth)
-void stream_copy(void* dst, const void* src, size_t bytes) {
+// pageable <-> pinned copy with non-temporal stores where aligned and `nt` (the destination
+// is not read back by this thread, so skipping its read-for-ownership saves host bandwidth);
+// with nt = false, ordinary stores leave the staged chunk in the last-level cache, where the
+// copy engine's read may find it
+void stream_copy(void* dst, const void* src, size_t bytes, bool nt = true) {
 #if defined(__x86_64__)
-    if (((uintptr_t)dst & 15) == 0 && (bytes & 15) == 0) {
+    if (nt && ((uintptr_t)dst & 15) == 0 && (bytes & 15) == 0) {
         __m128i* d = static_cast<__m128i*>(dst);
         const __m128i* s = static_cast<const __m128i*>(src);
         const size_t n = bytes / 16;
@@ -380,8 +382,11 @@ void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body) {
 double Engine::tune_host_pipeline(int reps) {
     if (!pool_) throw Unsupported("this context has no host pipeline");
     reps = std::max(1, reps);
+    // timing operand: pseudo-random limbs with the top limb of every coefficient zero, so that
+    // each coefficient is below 2^(32(L-1)) < q (the kernels' bounds assume inputs below q)
     std::vector<uint32_t> a(plan_.coeff_words(), 0), c(plan_.coeff_words());
-    for (size_t i = 0; i < a.size(); ++i) a[i] = (uint32_t)(i * 2654435761u) >> 8;  // any in-range limbs
+    for (size_t i = 0; i < a.size(); ++i)
+        a[i] = (i % plan_.L == plan_.L - 1) ? 0u : (uint32_t)(i * 2654435761u);
     double best = 1e30;
     uint32_t bi = in_body_, bo = out_body_;
     const uint32_t cand[3] = {4, 8, 16};
@@ -419,6 +424,7 @@ void Engine::setup_host_pipeline() {
     cuda_check(cudaHostAlloc(&h_status_, 16, cudaHostAllocDefault), "cudaHostAlloc");
     *h_status_ = 0;
     profile_ = std::getenv("POLYMULT_PROFILE") != nullptr;
+    if (const char* e = std::getenv("POLYMULT_GATHER_STORES")) nt_gather_ = std::strcmp(e, "cached") != 0;
     for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
@@ -628,7 +634,7 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         pool_->run((int)ntasks, [&](int t) {
             const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
             for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r)
-                stream_copy(dst + r * seg, src[P] + ((size_t)r * ncols + ch.col0) * L, seg * 4);
+                stream_copy(dst + r * seg, src[P] + ((size_t)r * ncols + ch.col0) * L, seg * 4, nt_gather_);
         });
     };
     uint32_t* dR[2] = {d_ra_, d_rb_};

@@ -167,6 +167,7 @@ class Engine {
     std::vector<cudaEvent_t> ev_in_, ev_done_in_, ev_crt_, ev_out_;
     uint32_t* h_status_ = nullptr;  // pinned copy of the device status word, written after each run_host
     bool profile_ = false;          // POLYMULT_PROFILE: per-call host and device timeline on stderr
+    bool nt_gather_ = true;         // POLYMULT_GATHER_STORES=cached: ordinary stores when staging inputs
     std::vector<cudaEvent_t> trace_ev_;  // timing events of that timeline
     cudaEvent_t ev_row_a_ = nullptr, ev_fused_ = nullptr;
     std::unique_ptr<HostPool> pool_;

@@ -89,3 +89,28 @@ def test_null_arguments():
     assert lib.pm_run(None, None, None, None) == polymult.PM_ERR_INVALID
     assert lib.pm_sync(None) == polymult.PM_ERR_INVALID
     lib.pm_free(None)
+
+
+def test_batch_server_pipeline_argument_checks():
+    """Argument checks of the batch, server and pipeline-tuning entry points, which fail before
+    any CUDA call (so they hold on a machine without a GPU)."""
+    import polymult
+    lib = ensure_library()
+    out = ctypes.c_void_p()
+    assert lib.pm_batch_init(None, 0, 0, 0, 0, ctypes.byref(out)) == polymult.PM_ERR_INVALID
+    one = (polymult.PmBatchClass * 1)()
+    assert lib.pm_batch_init(one, 1, 0, 0, 0, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_batch_init(one, 1, 7, 0, 0, ctypes.byref(out)) == polymult.PM_ERR_INVALID
+    assert lib.pm_batch_init(one, 1, 0, 64, 0, ctypes.byref(out)) == polymult.PM_ERR_INVALID
+    assert "unknown flags" in lib.pm_last_error().decode()
+    assert lib.pm_batch_run(None, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_batch_sync(None) == polymult.PM_ERR_INVALID
+    lib.pm_batch_free(None)
+    assert lib.pm_server_init(64, 256, 8, None, None, 0, 1 << 30, 4, 2, 0, 0, ctypes.byref(out)) == \
+        polymult.PM_ERR_INVALID
+    assert "resident" in lib.pm_last_error().decode()
+    assert lib.pm_server_run(None, 0, None, None, None, None, None, None) == polymult.PM_ERR_INVALID
+    lib.pm_server_free(None)
+    assert lib.pm_tune_pipeline(None, 3, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_get_pipeline(None, None) == polymult.PM_ERR_INVALID
+
