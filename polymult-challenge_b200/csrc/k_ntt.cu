@@ -242,7 +242,7 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
 //                  transform ra_sel[z] of RA when ra_sel is given (a server's resident
 //                  operands), else with transform z.
 template <int NB, bool FUSED>
-__global__ void __launch_bounds__(128) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
+__global__ void __launch_bounds__(128, 8) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
                                                   const uint32_t* __restrict__ ra_sel) {
     using C = RowCfg<NB>;
     __shared__ __align__(16) uint32_t sh[C::NPH > 1 ? 128 * C::E : 4];

@@ -142,177 +142,6 @@ __device__ __forceinline__ void bulk_g2s_all(void* dst, const void* src, uint32_
     }
 }
 
-}  // namespace
-
-// ----------------------------------------------------------------------------------------
-// Decomposition.  Persistent: grid <= #SMs, tiles of 128 positions over (batch, npos).
-// 256 threads = 8 epilogue warps; warp w reads TMEM lanes 32 (w % 4) of column half w / 4.
-// Per tile: the raw coefficients (contiguous cnt*L words) arrive by one bulk copy into a
-// double-buffered ring, prefetched two tiles ahead; all warps re-lay them out as the K-major
-// A operand; thread 0 issues the MMAs of the two prime halves with one commit each, so the
-// epilogue of half 0 overlaps the MMA of half 1.  512 threads: warp w reads TMEM lane quarter
-// w % 4 of prime half (w / 4) % 2, and of that half's 16-column chunks those with index
-// parity w / 8 -- four warps per lane quarter, so that the REDC epilogue (the longest phase)
-// has 16 warps to hide its latencies.
-// smem: [B image][A tile][raw ring 2 x 128*L words][bars: B, raw0, raw1, mma0, mma1][slot]
-// ----------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const uint32_t* __restrict__ src, ChunkMap C,
-                                                   uint32_t npos, uint32_t nbatch, uint32_t* __restrict__ R,
-                                                   int use_bulk) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    const int L = P.L, kb = P.dec_kbytes, nrows_b = P.dec_nrows;
-    const int KH = dec_half_primes(P.KP);                 // primes of half 0
-    const int n0 = 4 * KH, n1 = nrows_b - n0;              // MMA N of the halves
-    const uint32_t col1 = dec_half1_col(n0);               // TMEM column of half 1
-    unsigned char* b_s = smem_raw;
-    unsigned char* a_s = b_s + (size_t)nrows_b * kb;
-    uint32_t* raw_s = reinterpret_cast<uint32_t*>(a_s + (size_t)TC_M * kb);
-    const size_t raw_words = (size_t)TC_M * L;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(raw_s + 2 * raw_words);
-    uint64_t *bar_b = bars, *bar_raw = bars + 1, *bar_mma = bars + 3;
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 5);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t ncols = tmem_cols_for((int)col1 + n1);
-
-    const uint32_t tiles_per_batch = (npos + TC_M - 1) / TC_M;
-    const uint32_t ntiles = tiles_per_batch * nbatch;
-    auto tile_src = [&](uint32_t tile, int* cnt) {
-        const uint32_t b = tile / tiles_per_batch;
-        const uint32_t pos0 = (tile - b * tiles_per_batch) * TC_M;
-        *cnt = (int)min((uint32_t)TC_M, npos - pos0);
-        return src + ((size_t)b * npos + pos0) * L;
-    };
-
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < 5; ++i) mbar_init(bars + i, 1);
-        bulk_g2s_all(b_s, P.dec_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
-        if (use_bulk)
-            for (int k = 0; k < 2; ++k) {
-                const uint32_t t = blockIdx.x + k * gridDim.x;
-                if (t < ntiles) {
-                    int cnt;
-                    const uint32_t* s = tile_src(t, &cnt);
-                    bulk_g2s_all(raw_s + k * raw_words, s, (uint32_t)cnt * L * 4, bar_raw + k);
-                }
-            }
-    }
-    if (warp == 0) tmem_alloc(slot, ncols);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *slot;
-    bool ok = mbar_wait_bounded(bar_b, 0);
-
-    const uint32_t sbo = 8u * (uint32_t)kb;
-    const int groups = kb / 16;
-    const int half = (warp >> 2) & 1, sub = warp >> 3, m = (warp & 3) * 32 + lane;
-    uint32_t i = 0;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
-        const int buf = (int)(i & 1);
-        int cnt;
-        const uint32_t* s = tile_src(tile, &cnt);
-        uint32_t* raw = raw_s + buf * raw_words;
-        if (use_bulk) {
-            ok = ok && mbar_wait_bounded(bar_raw + buf, (i >> 1) & 1);
-        } else {
-            for (int w = threadIdx.x; w < cnt * L; w += blockDim.x) raw[w] = __ldg(s + w);
-        }
-        if (__syncthreads_or(!ok)) break;
-        // re-layout: row mm, 16-byte group g = limbs 4g..4g+3 (zero past L or past cnt)
-        for (int w = threadIdx.x; w < TC_M * groups; w += blockDim.x) {
-            const int mm = w & (TC_M - 1), g = w >> 7;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (mm < cnt) {
-                const uint32_t* row = raw + mm * L;
-                const int l0 = 4 * g;
-                v.x = l0 < L ? row[l0] : 0u;
-                v.y = l0 + 1 < L ? row[l0 + 1] : 0u;
-                v.z = l0 + 2 < L ? row[l0 + 2] : 0u;
-                v.w = l0 + 3 < L ? row[l0 + 3] : 0u;
-            }
-            *reinterpret_cast<uint4*>(a_s + (size_t)(mm >> 3) * sbo + (size_t)g * 128 + (mm & 7) * 16) = v;
-        }
-        fence_smem_to_async();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const uint32_t nxt = tile + 2 * gridDim.x;
-            if (use_bulk && nxt < ntiles) {  // the ring slot was just consumed
-                int c2;
-                const uint32_t* s2 = tile_src(nxt, &c2);
-                bulk_g2s_all(raw, s2, (uint32_t)c2 * L * 4, bar_raw + buf);
-            }
-            tc_fence_after();
-            issue_gemm_rows(tmem, smem_addr(a_s), smem_addr(b_s), 0, n0, kb);
-            umma_commit(bar_mma);
-            if (n1 > 0) {
-                issue_gemm_rows(tmem + col1, smem_addr(a_s), smem_addr(b_s), n0, n1, kb);
-                umma_commit(bar_mma + 1);
-            }
-        }
-        if (half == 0 || n1 > 0) {
-            // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
-            const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(bar_mma + half, i & 1));
-            if (!got) flag_error(P.status, DEV_ERR_WAIT);
-            tc_fence_after();
-            const uint32_t b = tile / tiles_per_batch;
-            const uint32_t pos0 = (tile - b * tiles_per_batch) * TC_M;
-            const uint32_t n = m < cnt ? chunk_pos_to_n(P, C, pos0 + m) : 0;
-            uint32_t* Rb = R + (size_t)b * P.K * P.N + n;
-            const int j0 = half ? KH : 0;
-            const int cols = half ? n1 : n0;
-            const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
-            for (int c16 = sub; c16 < cols / 16 && got; c16 += 2) {
-                uint32_t r[16];
-                tmem_ld16(tcol + (uint32_t)(16 * c16), r);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int j = j0 + 4 * c16 + q;
-                    if (j < P.K && m < cnt) {
-                        const uint64_t x = (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
-                                           ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24);
-                        const uint32_t p = __ldg(P.p + j);
-                        Rb[(size_t)j * P.N] = red_once(redc64(x, p, __ldg(P.pinv + j)), p);
-                    }
-                }
-            }
-            ok = ok && got;
-        }
-        tc_fence_before();
-        if (__syncthreads_or(!ok)) break;
-    }
-    if (!ok && threadIdx.x == 0) flag_error(P.status, DEV_ERR_WAIT);
-    __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, ncols);
-}
-
-// ----------------------------------------------------------------------------------------
-// CRT.  Persistent, warp-specialised, 512 threads:
-//   producers (warps 0-7, two threads per coefficient m = t % 128, each half of the prime
-//     groups): load the tile's residues straight from global memory, y_j = x_j (M/p_j)^-1
-//     mod p_j into registers, fp32 partial sums of y_j / p_j; then wait until the previous
-//     tile's MMA has read the A tile, write the y bytes as the K-major A operand, and one
-//     thread issues the tile's MMAs into TMEM accumulator i % 2 (N = result bytes,
-//     K = 4 KP bytes) and commits them;
-//   epilogue (warps 8-15, two threads per coefficient, TMEM lane quarter warp % 4): for tile
-//     i, wait for its accumulator, v = round(sum y_j / p_j), accumulator bytes -> limbs with
-//     carries + T_v into a staging row, release the accumulator, carry merge, delta fold,
-//     - q, coalesced store.
-// With two accumulators the epilogue of tile i overlaps the loads, prologue and MMA of tile
-// i + 1.  Hand-offs: mbarriers mma_done[2] (tcgen05.commit), acc_empty[2] (256 epilogue
-// arrivals), v_ready[2] (one producer arrival after the producers' barrier, releasing the
-// partial sums); named barriers 1 (producers) and 2 (epilogue).  Every wait is bounded: a
-// wait that runs out sets a shared abort flag that ends both loops (agreed per group with a
-// barrier reduction), the status word gets DEV_ERR_WAIT, and the kernel waits (bounded) for
-// its own copies and MMAs in flight before it frees TMEM.
-// smem: [B image][A tile][z staging 128 x zs][per-prime constants KP x uint4]
-//       [partial sums 2 x 2 x 128 f32][bars: b, mma_done 2, acc_empty 2, v_ready 2][slot][abort]
-// ----------------------------------------------------------------------------------------
-namespace {
-
-constexpr int CRT_PROD_THREADS = 256;
-constexpr int CRT_EPI_THREADS = 256;
-constexpr int CRT_BATCH_GROUPS = 3;      // prime groups (4 primes each) per batch of producer loads
-
 __device__ __forceinline__ void named_sync(int id, int n) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
@@ -348,6 +177,207 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
     }
     return true;
 }
+
+}  // namespace
+
+// ----------------------------------------------------------------------------------------
+// Decomposition.  Persistent, warp-specialised, 640 threads; tiles of 128 positions over
+// (batch, npos).
+//   loader group (warps 0-3): thread 0 keeps a 2-deep ring of raw coefficient tiles filled by
+//     bulk copies (contiguous cnt*L words each, prefetched two tiles ahead); the group
+//     re-lays the tile out as the K-major A operand once the previous tile's MMAs have read
+//     A; thread 0 then issues the MMAs of the two prime halves -- half h once the epilogue
+//     has released TMEM half h -- with one commit per half (mma_done[h]);
+//   epilogue group (warps 4-19): warp w reads TMEM lane quarter w % 4 of prime half
+//     ((w - 4) / 4) % 2, the 16-column chunks of parity (w - 4) / 8, and turns four byte
+//     columns into a 64-bit sum, one REDC and a residue store; the 256 threads of a half
+//     arrive on acc_empty[h] when they have read it.
+// So tile i's epilogue (the long phase) overlaps tile i+1's copy, relayout and MMAs.  Bounded
+// waits with a shared abort flag as in the CRT kernel.
+// smem: [B image][A tile][raw ring 2 x 128*L words][bars: B, raw 2, mma_done 2, acc_empty 2]
+//       [slot][abort]
+// ----------------------------------------------------------------------------------------
+constexpr int DEC_LOAD_THREADS = 128;
+constexpr int DEC_EPI_THREADS = 512;
+
+__global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const uint32_t* __restrict__ src, ChunkMap C,
+                                                              uint32_t npos, uint32_t nbatch, uint32_t* __restrict__ R,
+                                                              int use_bulk) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int L = P.L, kb = P.dec_kbytes, nrows_b = P.dec_nrows;
+    const int KH = dec_half_primes(P.KP);                 // primes of half 0
+    const int n0 = 4 * KH, n1 = nrows_b - n0;              // MMA N of the halves
+    const uint32_t col1 = dec_half1_col(n0);               // TMEM column of half 1
+    unsigned char* b_s = smem_raw;
+    unsigned char* a_s = b_s + (size_t)nrows_b * kb;
+    uint32_t* raw_s = reinterpret_cast<uint32_t*>(a_s + (size_t)TC_M * kb);
+    const size_t raw_words = (size_t)TC_M * L;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(raw_s + 2 * raw_words);
+    uint64_t *bar_b = bars, *bar_raw = bars + 1, *mma_done = bars + 3, *acc_empty = bars + 5;
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 7);
+    volatile int* abort_f = reinterpret_cast<volatile int*>(slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t ncols = tmem_cols_for((int)col1 + n1);
+    const int nhalves = n1 > 0 ? 2 : 1;
+
+    const uint32_t tiles_per_batch = (npos + TC_M - 1) / TC_M;
+    const uint32_t ntiles = tiles_per_batch * nbatch;
+    auto tile_src = [&](uint32_t tile, int* cnt) {
+        const uint32_t b = tile / tiles_per_batch;
+        const uint32_t pos0 = (tile - b * tiles_per_batch) * TC_M;
+        *cnt = (int)min((uint32_t)TC_M, npos - pos0);
+        return src + ((size_t)b * npos + pos0) * L;
+    };
+
+    if (threadIdx.x == 0) {
+        mbar_init(bar_b, 1);
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(bar_raw + k, 1);
+            mbar_init(mma_done + k, 1);
+            mbar_init(acc_empty + k, DEC_EPI_THREADS / 2);
+        }
+        *abort_f = 0;
+        bulk_g2s_all(b_s, P.dec_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
+        if (use_bulk)
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t t = blockIdx.x + k * gridDim.x;
+                if (t < ntiles) {
+                    int cnt;
+                    const uint32_t* s = tile_src(t, &cnt);
+                    bulk_g2s_all(raw_s + k * raw_words, s, (uint32_t)cnt * L * 4, bar_raw + k);
+                }
+            }
+    }
+    if (warp == 0) tmem_alloc(slot, ncols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    // thread 0's record of what is in flight, for the abort path: the last commit (barrier and
+    // phase parity) and, per ring slot, a bulk copy nobody has waited for (and its parity)
+    int last_commit = -1;
+    uint32_t last_commit_par = 0;
+    bool b_seen = false;
+    uint32_t raw_pending = 0, raw_par = 0;
+    if (threadIdx.x == 0 && use_bulk)
+        for (int k = 0; k < 2; ++k)
+            if (blockIdx.x + k * gridDim.x < ntiles) raw_pending |= 1u << k;  // parity 0
+
+    if (threadIdx.x < DEC_LOAD_THREADS) {
+        // ---------------- loader / relayout / MMA issue ----------------
+        const uint32_t sbo = 8u * (uint32_t)kb;
+        const int groups = kb / 16;
+        uint32_t i = 0;
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            if (named_sync_or(1, DEC_LOAD_THREADS, *abort_f != 0)) break;
+            const int buf = (int)(i & 1);
+            int cnt;
+            const uint32_t* s = tile_src(tile, &cnt);
+            uint32_t* raw = raw_s + buf * raw_words;
+            if (use_bulk) {
+                if (wait_or_abort(bar_raw + buf, (i >> 1) & 1, abort_f) && threadIdx.x == 0) raw_pending &= ~(1u << buf);
+            } else {
+                for (int w = threadIdx.x; w < cnt * L; w += DEC_LOAD_THREADS) raw[w] = __ldg(s + w);
+            }
+            // the previous tile's MMAs must have read A (mma_done of its last half)
+            if (i > 0) wait_or_abort(mma_done + (nhalves - 1), (i - 1) & 1, abort_f);
+            named_sync(1, DEC_LOAD_THREADS);  // raw tile visible to the whole group
+            // re-layout: row mm, 16-byte group g = limbs 4g..4g+3 (zero past L or past cnt)
+            for (int w = threadIdx.x; w < TC_M * groups; w += DEC_LOAD_THREADS) {
+                const int mm = w & (TC_M - 1), g = w >> 7;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (mm < cnt) {
+                    const uint32_t* row = raw + mm * L;
+                    const int l0 = 4 * g;
+                    v.x = l0 < L ? row[l0] : 0u;
+                    v.y = l0 + 1 < L ? row[l0 + 1] : 0u;
+                    v.z = l0 + 2 < L ? row[l0 + 2] : 0u;
+                    v.w = l0 + 3 < L ? row[l0 + 3] : 0u;
+                }
+                *reinterpret_cast<uint4*>(a_s + (size_t)(mm >> 3) * sbo + (size_t)g * 128 + (mm & 7) * 16) = v;
+            }
+            fence_smem_to_async();
+            named_sync(1, DEC_LOAD_THREADS);
+            if (threadIdx.x == 0) {
+                const uint32_t nxt = tile + 2 * gridDim.x;
+                if (use_bulk && nxt < ntiles) {  // the ring slot was just consumed
+                    int c2;
+                    const uint32_t* s2 = tile_src(nxt, &c2);
+                    bulk_g2s_all(raw, s2, (uint32_t)c2 * L * 4, bar_raw + buf);
+                    raw_pending |= 1u << buf;
+                    raw_par = (raw_par & ~(1u << buf)) | ((((i + 2) >> 1) & 1u) << buf);
+                }
+                bool ok = *abort_f == 0;
+                if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, abort_f);
+                for (int h = 0; h < nhalves && ok; ++h) {
+                    if (i > 0) ok = wait_or_abort(acc_empty + h, (i - 1) & 1, abort_f);
+                    if (!ok) break;
+                    tc_fence_after();
+                    if (h == 0) issue_gemm_rows(tmem, smem_addr(a_s), smem_addr(b_s), 0, n0, kb);
+                    else issue_gemm_rows(tmem + col1, smem_addr(a_s), smem_addr(b_s), n0, n1, kb);
+                    umma_commit(mma_done + h);
+                    last_commit = h;
+                    last_commit_par = i & 1;
+                }
+            }
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        const int we = warp - DEC_LOAD_THREADS / 32;
+        const int half = (we >> 2) & 1, sub = we >> 3, m = (warp & 3) * 32 + lane;
+        const bool active = half < nhalves;
+        uint32_t i = 0;
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            if (named_sync_or(2, DEC_EPI_THREADS, *abort_f != 0)) break;
+            if (!active) continue;
+            int cnt;
+            (void)tile_src(tile, &cnt);
+            // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
+            const bool got = __all_sync(0xffffffffu, wait_or_abort(mma_done + half, i & 1, abort_f));
+            tc_fence_after();
+            const uint32_t b = tile / tiles_per_batch;
+            const uint32_t pos0 = (tile - b * tiles_per_batch) * TC_M;
+            const uint32_t n = m < cnt ? chunk_pos_to_n(P, C, pos0 + m) : 0;
+            uint32_t* Rb = R + (size_t)b * P.K * P.N + n;
+            const int j0 = half ? KH : 0;
+            const int cols = half ? n1 : n0;
+            const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
+            for (int c16 = sub; c16 < cols / 16 && got; c16 += 2) {
+                uint32_t r[16];
+                tmem_ld16(tcol + (uint32_t)(16 * c16), r);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int j = j0 + 4 * c16 + q;
+                    if (j < P.K && m < cnt) {
+                        const uint64_t x = (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
+                                           ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24);
+                        const uint32_t p = __ldg(P.p + j);
+                        Rb[(size_t)j * P.N] = red_once(redc64(x, p, __ldg(P.pinv + j)), p);
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(acc_empty + half);  // this thread has read TMEM half `half` of tile i
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_f) {
+        flag_error(P.status, DEV_ERR_WAIT);
+        // copies and MMAs still in flight must land before this CTA's memory goes away
+        if (!b_seen) mbar_wait_bounded(bar_b, 0);
+        for (int k = 0; k < 2; ++k)
+            if (raw_pending & (1u << k)) mbar_wait_bounded(bar_raw + k, (raw_par >> k) & 1u);
+        if (last_commit >= 0) mbar_wait_bounded(mma_done + last_commit, last_commit_par);
+    }
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+namespace {
+
+constexpr int CRT_PROD_THREADS = 256;
+constexpr int CRT_EPI_THREADS = 256;
+constexpr int CRT_BATCH_GROUPS = 3;      // prime groups (4 primes each) per batch of producer loads
 
 struct CrtSmem {
     unsigned char* b;
@@ -583,7 +613,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
 }
 
 size_t rns_tc_smem(const DevPlan& P) {
-    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + 2 * (size_t)TC_M * P.L * 4 + 64;
+    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + 2 * (size_t)TC_M * P.L * 4 + 7 * 8 + 16;
 }
 
 size_t crt_tc_smem(const DevPlan& P) {

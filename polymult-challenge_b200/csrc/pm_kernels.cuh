@@ -41,7 +41,7 @@ constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
 __global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R,
                          int use_bulk);
 __global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out);
-constexpr int RNS_TC_THREADS = 512;  // 16 epilogue warps: 4 TMEM lane quarters x 2 prime halves x 2 column sets
+constexpr int RNS_TC_THREADS = 640;  // 4 loader warps + 16 epilogue warps (4 lane quarters x 2 prime halves x 2 column sets)
 constexpr int CRT_TC_THREADS = 512;  // 256 producers + 256 epilogue threads, two per coefficient each
 size_t rns_tc_smem(const DevPlan& P);
 size_t crt_tc_smem(const DevPlan& P);
