@@ -452,6 +452,9 @@ def run_ours(args):
     import workload
     world, rank, local = dist_init()
     torch.cuda.set_device(local)
+    # torch's CPU thread pool stays at one thread: the host pipeline's staging threads need the
+    # cores (the bench does no CPU tensor work)
+    torch.set_num_threads(1)
     N, W = N_RANK, W_RANK
     L = (W + 31) // 32
     q = workload.spec_prime(N, W)
