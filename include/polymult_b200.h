@@ -40,14 +40,17 @@ enum pm_status {
 enum pm_gemm_form {
     PM_GEMM_AUTO = 0,   /* tensor cores where the point fits, else CUDA cores */
     PM_GEMM_PLAIN = 1,  /* int32 CUDA-core kernels */
-    PM_GEMM_TENSOR = 2  /* tcgen05 kind::i8 byte-sliced GEMMs (error if the point does not fit) */
+    PM_GEMM_TENSOR = 2, /* tcgen05 kind::i8 byte-sliced GEMMs (error if the point does not fit) */
+    PM_GEMM_MIXED = 3   /* tensor-core decomposition (in prime blocks where K > 128), CUDA-core
+                           CRT; also what PM_GEMM_AUTO resolves to where only the decomposition
+                           fits the tensor-core kernels */
 };
 
 typedef struct pm_info {
     uint32_t N, W, L;
     int32_t K;             /* RNS primes */
     int32_t logN, w1, w2;  /* 4-step split: nrows = 2^w1, ncols = 2^w2 */
-    int32_t gemm_form;     /* resolved form: PM_GEMM_PLAIN or PM_GEMM_TENSOR */
+    int32_t gemm_form;     /* resolved form: PM_GEMM_PLAIN, PM_GEMM_TENSOR or PM_GEMM_MIXED */
     int32_t device;
     uint64_t delta;        /* 2^W - q */
     uint64_t table_bytes;  /* device memory of the per-point tables */

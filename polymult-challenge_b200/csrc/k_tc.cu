@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
             const uint32_t b = tile / tiles_per_batch;
             const uint32_t pos0 = (tile - b * tiles_per_batch) * TC_M;
             const uint32_t n = m < cnt ? chunk_pos_to_n(P, C, pos0 + m) : 0;
-            uint32_t* Rb = R + (size_t)b * P.K * P.N + n;
+            uint32_t* Rb = R + (size_t)b * P.Kr * P.N + n;
             const int j0 = half ? KH : 0;
             const int cols = half ? n1 : n0;
             const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
@@ -409,9 +409,13 @@ __device__ __forceinline__ CrtSmem crt_smem(unsigned char* base, const DevPlan& 
 
 __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const uint32_t* __restrict__ R, ChunkMap C,
                                                               uint32_t npos, uint32_t nbatch,
-                                                              uint32_t* __restrict__ out) {
+                                                              uint32_t* __restrict__ out, CrtPartial part) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const CrtSmem S = crt_smem(smem_raw, P);
+    // partial modes: the block's integer (and, if add_s, its share of sum y_j / p_j) goes into
+    // the per-coefficient partial buffers instead of the output; zp_s stages a tile of them
+    uint32_t* zp_s = S.slot + 8;  // after [slot][abort] and padding: 32 bytes past the barriers
+    const int zlt = crt_zl(P.L);
     uint64_t *bar_b = S.bars, *mma_done = S.bars + 1, *acc_empty = S.bars + 3, *v_ready = S.bars + 5;
     const int K = P.K, KP = P.KP, L = P.L, kb = P.crt_kbytes, nrows_b = P.crt_nrows;
     const int zl = crt_zl(L), zs = crt_zstride(L);
@@ -454,7 +458,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             const uint32_t bt = tile / tiles_per_batch;
             const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
             const bool valid = (uint32_t)m < npos - pos0;
-            const uint32_t* Rm = R + (size_t)bt * K * P.N + (valid ? chunk_pos_to_n(P, C, pos0 + m) : 0u);
+            const uint32_t* Rm = R + (size_t)bt * P.Kr * P.N + (valid ? chunk_pos_to_n(P, C, pos0 + m) : 0u);
             // residues in batches of CRT_BATCH_GROUPS groups (4 primes each), the next batch's
             // loads in flight while this batch is converted: up to 2 x 16 loads per thread
             float s4[4] = {0.f, 0.f, 0.f, 0.f};
@@ -538,8 +542,12 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             tc_fence_after();
             const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
             const float vf = rintf(sum);
-            if (hf == 0 && valid && got && fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
-            const int v = min(max((int)vf, 0), K);
+            if (part.mode == CRT_FULL && hf == 0 && valid && got && fabsf(sum - vf) > 0.25f)
+                flag_error(P.status, DEV_ERR_CRT_BOUND);
+            const int v = part.mode == CRT_FULL ? min(max((int)vf, 0), K) : 0;
+            const size_t gpos = (size_t)bt * npos + pos0;  // first coefficient of the tile in the partial buffers
+            if (part.mode != CRT_FULL && part.add_s && hf == 0 && valid)
+                part.sp[gpos + m] = (part.mode == CRT_PARTIAL_FIRST ? 0.f : part.sp[gpos + m]) + sum;
             // accumulator bytes -> limbs with carries, + v T_1 (T_1 = (-M) mod q; v T_1 == T_v mod q,
             // < 2^(W+7), and the fold below reduces it; one row for every lane instead of a
             // per-lane row T_v); half hf owns limbs [0, lh) or [lh, zl)
@@ -571,6 +579,16 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             }
             tc_fence_before();
             mbar_arrive(acc_empty + b);  // accumulator b and partial sums b are free again
+            if (part.mode != CRT_FULL) {
+                // stage the tile's partial rows (zeros for the first block), add this block's
+                // integer at limb offset limb0 with one carry chain per coefficient, store back
+                uint32_t* zg = part.zp + gpos * zlt;
+                for (int w = et; w < TC_M * zlt; w += CRT_EPI_THREADS) {
+                    const int mm = w / zlt;
+                    zp_s[(size_t)mm * zs + (w - mm * zlt)] =
+                        (part.mode == CRT_PARTIAL_FIRST || mm >= cnt) ? 0u : zg[w];
+                }
+            }
             named_sync(2, CRT_EPI_THREADS);
             if (hf == 0 && valid) {
                 for (int k = lh; carry && k < zl; ++k) {  // half 0's carry-out into half 1's limbs
@@ -578,9 +596,33 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                     z[k] = (uint32_t)t;
                     carry = t >> 32;
                 }
-                crt_reduce_mod_q(z, zl, P);
+                if (part.mode == CRT_FULL) {
+                    crt_reduce_mod_q(z, zl, P);
+                } else {
+                    uint32_t* zr = zp_s + (size_t)m * zs;
+                    uint64_t c2 = 0;
+                    int k = part.limb0;
+                    for (int l2 = 0; l2 < zl && k < zlt; ++l2, ++k) {
+                        const uint64_t t = (uint64_t)zr[k] + z[l2] + c2;
+                        zr[k] = (uint32_t)t;
+                        c2 = t >> 32;
+                    }
+                    for (; c2 && k < zlt; ++k) {
+                        const uint64_t t = (uint64_t)zr[k] + c2;
+                        zr[k] = (uint32_t)t;
+                        c2 = t >> 32;
+                    }
+                }
             }
             named_sync(2, CRT_EPI_THREADS);
+            if (part.mode != CRT_FULL) {
+                uint32_t* zg = part.zp + gpos * zlt;
+                for (int w = et; w < cnt * zlt; w += CRT_EPI_THREADS) {
+                    const int mm = w / zlt;
+                    zg[w] = zp_s[(size_t)mm * zs + (w - mm * zlt)];
+                }
+                continue;
+            }
             // coalesced store of the tile's cnt x L limbs (contiguous in the output)
             uint32_t* o = out + ((size_t)bt * npos + pos0) * L;
             const int tot = cnt * L;
@@ -616,9 +658,49 @@ size_t rns_tc_smem(const DevPlan& P) {
     return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + 2 * (size_t)TC_M * P.L * 4 + 7 * 8 + 16;
 }
 
-size_t crt_tc_smem(const DevPlan& P) {
+size_t crt_tc_smem(const DevPlan& P, bool partial) {
     return (size_t)P.crt_nrows * P.crt_kbytes + (size_t)TC_M * P.crt_kbytes + crt_z_bytes(P) + (size_t)P.KP * 16 +
-           4 * TC_M * 4 + 7 * 8 + 16;
+           4 * TC_M * 4 + 7 * 8 + 32 + (partial ? crt_z_bytes(P) : 0);
+}
+
+// Last step of a CRT computed in blocks: per coefficient, v = round(sum of the blocks'
+// partial sums of y_j / p_j) with the |x| < M/8 check, z = partial integer + v T_1, delta fold,
+// - q; 128 threads, one coefficient each, rows staged through shared memory so that loads and
+// stores are coalesced.
+__global__ void __launch_bounds__(TC_M) k_crt_finish(DevPlan P, const uint32_t* __restrict__ zp,
+                                                    const float* __restrict__ sp, uint32_t total,
+                                                    uint32_t* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int L = P.L, zl = crt_zl(L), zs = crt_zstride(L);
+    uint32_t* zrow = reinterpret_cast<uint32_t*>(smem_raw);  // [128][zs]
+    const size_t c0 = (size_t)blockIdx.x * TC_M;
+    const int cnt = (int)min((size_t)TC_M, total - c0);
+    for (int w = threadIdx.x; w < cnt * zl; w += TC_M) {
+        const int mm = w / zl;
+        zrow[(size_t)mm * zs + (w - mm * zl)] = zp[c0 * zl + w];
+    }
+    __syncthreads();
+    const int m = threadIdx.x;
+    if (m < cnt) {
+        const float sum = sp[c0 + m];
+        const float vf = rintf(sum);
+        if (fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
+        const uint32_t v = (uint32_t)min(max((int)vf, 0), P.K);
+        uint32_t* z = zrow + (size_t)m * zs;
+        const uint32_t* T1 = P.tneg + L;
+        uint64_t carry = 0;
+        for (int l = 0; l < zl; ++l) {
+            const uint64_t t = (uint64_t)z[l] + carry + (l < L ? (uint64_t)v * __ldg(T1 + l) : 0ull);
+            z[l] = (uint32_t)t;
+            carry = t >> 32;
+        }
+        crt_reduce_mod_q(z, zl, P);
+    }
+    __syncthreads();
+    for (int w = threadIdx.x; w < cnt * L; w += TC_M) {
+        const int mm = w / L;
+        out[c0 * L + w] = zrow[(size_t)mm * zs + (w - mm * L)];
+    }
 }
 
 }  // namespace pm

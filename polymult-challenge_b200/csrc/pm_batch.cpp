@@ -166,7 +166,8 @@ void Batch::choose_configs(int gemm_request) {
             int logN = 0;
             while ((1u << logN) < s.N) ++logN;
             std::vector<std::pair<int, int>> cand;
-            const int forms[2] = {GEMM_TENSOR, GEMM_PLAIN};
+            // AUTO resolves to the tensor-core form, or the mixed one where the CRT does not fit
+            const int forms[2] = {GEMM_AUTO, GEMM_PLAIN};
             for (int f : forms) {
                 if (gemm_request != GEMM_AUTO && f != gemm_request) continue;
                 for (int w1 = logN / 2 - 1; w1 <= logN / 2 + 1; ++w1)
@@ -187,6 +188,7 @@ void Batch::choose_configs(int gemm_request) {
                 } catch (const InvalidPoint&) {
                     continue;
                 }
+                e->reserve((size_t)s.count * e->plan().N);
                 const size_t words = (size_t)s.count * e->plan().K * e->plan().N;
                 if (probe) cudaFree(probe);
                 probe = nullptr;
@@ -251,6 +253,7 @@ void Batch::alloc_scratch() {
     };
     std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return work(x) > work(y); });
     const size_t ns = std::max<size_t>(1, std::min<size_t>(kMaxStreams, cls_.size()));
+    for (auto& c : cls_) c.eng->reserve((size_t)c.src.count * c.eng->plan().N);
     std::vector<double> load(ns, 0.0);
     std::vector<size_t> need(ns, 0);
     sched_.assign(ns, {});

@@ -54,7 +54,7 @@ extern "C" {
 int pm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_form, int device, pm_context** out) {
     if (!out) return fail(PM_ERR_INVALID, "out is null");
     *out = nullptr;
-    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_TENSOR) return fail(PM_ERR_INVALID, "bad gemm_form");
+    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_MIXED) return fail(PM_ERR_INVALID, "bad gemm_form");
     return guarded([&] {
         pm::Engine* e = new pm::Engine(N, W, L, q, gemm_form, device);
         try {
@@ -152,7 +152,7 @@ int pm_batch_init(const pm_batch_class* classes, uint32_t nclasses, int gemm_for
     if (!out) return fail(PM_ERR_INVALID, "out is null");
     *out = nullptr;
     if (!classes || nclasses == 0) return fail(PM_ERR_INVALID, "no classes");
-    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_TENSOR) return fail(PM_ERR_INVALID, "bad gemm_form");
+    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_MIXED) return fail(PM_ERR_INVALID, "bad gemm_form");
     if (flags & ~(PM_BATCH_TUNE | PM_BATCH_NO_GRAPH)) return fail(PM_ERR_INVALID, "unknown flags");
     return guarded([&] { *out = new pm_batch{new pm::Batch(classes, nclasses, gemm_form, flags, device)}; });
 }
@@ -205,7 +205,7 @@ int pm_server_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const 
     if (!out) return fail(PM_ERR_INVALID, "out is null");
     *out = nullptr;
     if (!resident || nresident == 0) return fail(PM_ERR_INVALID, "no resident operands");
-    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_TENSOR) return fail(PM_ERR_INVALID, "bad gemm_form");
+    if (gemm_form < PM_GEMM_AUTO || gemm_form > PM_GEMM_MIXED) return fail(PM_ERR_INVALID, "bad gemm_form");
     return guarded([&] {
         *out = new pm_server{
             new pm::Server(N, W, L, q, resident, nresident, hbm_budget, max_batch, streams, gemm_form, device)};

@@ -26,6 +26,7 @@ struct DevPlan {
     uint32_t N, nrows, ncols;
     int logN, w1, w2;
     int K, KP, L, W, HP;
+    int Kr;                   // primes of the residue arrays R[batch][Kr][N] (K except in a prime block)
     uint64_t delta;
     const uint32_t* p;        // [KP]
     const uint32_t* pinv;     // [KP] p^-1 mod 2^32

@@ -245,15 +245,27 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
     try {
         upload_tables();
         setup_launch_shapes();
-        const bool tc_fits = rns_tc_smem(dp_) <= smem_optin_ && crt_tc_smem(dp_) <= smem_optin_ &&
-                             plan_.KP <= 128 && dp_.crt_nrows <= 256;
-        if (gemm_request == GEMM_TENSOR && !tc_fits)
+        // The tensor-core decomposition runs in prime blocks of at most 128 primes (TMEM holds
+        // 4 byte columns per prime) whose B image fits shared memory; the tensor-core CRT needs
+        // every prime in one tile (K <= 128) and a result of at most 256 bytes.  Points beyond
+        // the CRT's reach (K > 128: W above about 1900 bits) take the mixed form: tensor-core
+        // decomposition, CUDA-core CRT.
+        const bool dec_fits = make_dec_blocks();
+        const bool crt_fits = crt_tc_smem(dp_) <= smem_optin_ && plan_.KP <= 128 && dp_.crt_nrows <= 256;
+        const bool crt_blocks = !crt_fits && dec_fits && make_crt_blocks();
+        if (gemm_request == GEMM_TENSOR && !(dec_fits && (crt_fits || crt_blocks)))
             throw Unsupported("tensor-core GEMM form does not cover this point (shared memory / TMEM)");
-        form_ = (gemm_request == GEMM_PLAIN || !tc_fits) ? GEMM_PLAIN : GEMM_TENSOR;
-        if (form_ == GEMM_TENSOR) {
-            smem_dec_ = rns_tc_smem(dp_);
-            smem_crt_ = crt_tc_smem(dp_);
+        if (gemm_request == GEMM_MIXED && !dec_fits)
+            throw Unsupported("tensor-core decomposition does not cover this point (shared memory)");
+        dec_tc_ = gemm_request != GEMM_PLAIN && dec_fits;
+        crt_tc_ = dec_tc_ && crt_fits && gemm_request != GEMM_MIXED;
+        crt_blocked_ = dec_tc_ && !crt_fits && crt_blocks && gemm_request != GEMM_MIXED;
+        form_ = (crt_tc_ || crt_blocked_) ? GEMM_TENSOR : dec_tc_ ? GEMM_MIXED : GEMM_PLAIN;
+        if (dec_tc_) {
+            smem_dec_ = 0;
+            for (const DecBlock& b : dec_blocks_) smem_dec_ = std::max(smem_dec_, b.smem);
         }
+        if (crt_tc_) smem_crt_ = crt_tc_smem(dp_);
         // multiplies per launch group of run_device: up to POLYMULT_GROUP_WORDS residue words
         // per operand (default 64 Mi: 8 multiplies at N = 65536, W = 1747, 512 MB of residue
         // scratch), at most 256.  Measured there: 1 multiply per group 4083 mults/s, 2 4789,
@@ -263,6 +275,7 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
         if (const char* e = std::getenv("POLYMULT_GROUP_WORDS")) group_words = std::max<size_t>(1, std::strtoull(e, nullptr, 10));
         const size_t per_mult = (size_t)plan_.K * plan_.N;
         group_cap_ = (uint32_t)std::max<size_t>(1, std::min<size_t>(256, group_words / std::max<size_t>(1, per_mult)));
+        if (crt_blocked_) reserve_crt_partials((size_t)group_cap_ * plan_.N);
         if (opt.host_pipeline) {
             ensure_scratch(1);
             setup_host_pipeline();
@@ -292,6 +305,8 @@ Engine::~Engine() {
     for (void* d : dev_allocs_) cudaFree(d);
     if (d_ra_) cudaFree(d_ra_);
     if (d_rb_) cudaFree(d_rb_);
+    if (d_zp_) cudaFree(d_zp_);
+    if (d_sp_) cudaFree(d_sp_);
     for (auto h : h_in_)
         if (h) cudaFreeHost(h);
     if (h_out_) cudaFreeHost(h_out_);
@@ -308,6 +323,7 @@ void Engine::upload_tables() {
     d.w1 = P.w1;
     d.w2 = P.w2;
     d.K = P.K;
+    d.Kr = P.K;
     d.KP = P.KP;
     d.L = (int)P.L;
     d.W = (int)P.W;
@@ -364,6 +380,7 @@ void Engine::setup_launch_shapes() {
     cuda_check(cudaFuncSetAttribute(k_crt_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_rns_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_crt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_crt_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
 }
 
 void Engine::ensure_scratch(uint32_t group) {
@@ -466,7 +483,105 @@ void Engine::setup_host_pipeline() {
     pool_.reset(new HostPool(workers));
 }
 
-int Engine::kernel_launches_per_group() const { return plan_.w1 > 0 ? 8 : 6; }
+// Prime blocks of the tensor-core decomposition: the largest block (a multiple of 4 primes,
+// at most 128) whose B image slice fits shared memory next to the A tile and the raw ring.
+// A block's B operand is a contiguous slice of the full image (rows 4j + t, 4 j0 a multiple
+// of 8); its kernel sees K = the block's primes, p / pinv from j0, and writes residue rows
+// j0.. of the full arrays.  False if no block fits.
+bool Engine::make_dec_blocks() {
+    dec_blocks_.clear();
+    int kpb = std::min(plan_.KP, 128) & ~3;
+    for (; kpb >= 4; kpb -= 4) {
+        DevPlan t = dp_;
+        t.KP = kpb;
+        t.dec_nrows = 4 * kpb;
+        if (rns_tc_smem(t) <= smem_optin_) break;
+    }
+    if (kpb < 4) return false;
+    for (int j0 = 0; j0 < plan_.K; j0 += kpb) {
+        DecBlock b;
+        b.j0 = (uint32_t)j0;
+        b.dp = dp_;
+        b.dp.K = std::min(kpb, plan_.K - j0);
+        b.dp.KP = (b.dp.K + 3) & ~3;
+        b.dp.p += j0;
+        b.dp.pinv += j0;
+        b.dp.dec_b += (size_t)4 * j0 * dp_.dec_kbytes;
+        b.dp.dec_nrows = 4 * b.dp.KP;
+        b.smem = rns_tc_smem(b.dp);
+        dec_blocks_.push_back(b);
+    }
+    return true;
+}
+
+// Blocks of a CRT whose primes do not fit one tile: prime blocks of the largest multiple of 4
+// (at most 128) and result-byte blocks of at most 256 bytes (TMEM columns) such that the
+// partial-mode kernel fits shared memory.  Each block gets its own B image -- rows v0.. of the
+// full image, K columns 4 j0.. -- re-packed into the canonical layout with the block's K width.
+bool Engine::make_crt_blocks() {
+    crt_blocks_.clear();
+    const int nrows_full = plan_.crt_gemm.n_rows, kb_full = plan_.crt_gemm.k_bytes;
+    auto round_up = [](int x, int m) { return (x + m - 1) / m * m; };
+    int kpb = std::min(plan_.KP, 128) & ~3;
+    for (; kpb >= 4; kpb -= 4) {
+        DevPlan t = dp_;
+        t.KP = kpb;
+        t.crt_kbytes = round_up(4 * kpb, 32);
+        t.crt_nrows = std::min(256, nrows_full);
+        if (crt_tc_smem(t, true) <= smem_optin_) break;
+    }
+    if (kpb < 4) return false;
+    for (int j0 = 0; j0 < plan_.K; j0 += kpb) {
+        const int cnt = std::min(kpb, plan_.K - j0), kp = (cnt + 3) & ~3, kb = round_up(4 * kp, 32);
+        for (int v0 = 0; v0 < nrows_full; v0 += 256) {
+            const int nr = std::min(256, nrows_full - v0);
+            std::vector<uint8_t> img((size_t)nr * kb, 0);
+            for (int v = 0; v < nr; ++v)
+                for (int kbyte = 0; kbyte < 4 * kp; ++kbyte) {
+                    const int fk = 4 * j0 + kbyte;
+                    if (fk < kb_full)
+                        img[umma_kmajor_offset(v, kbyte, kb)] = plan_.crt_b[umma_kmajor_offset(v0 + v, fk, kb_full)];
+                }
+            CrtBlock b;
+            b.j0 = (uint32_t)j0;
+            b.dp = dp_;
+            b.dp.K = cnt;
+            b.dp.KP = kp;
+            b.dp.p += j0;
+            b.dp.pinv += j0;
+            b.dp.crt_c += j0;
+            b.dp.crt_cc += j0;
+            b.dp.rcp += j0;
+            b.dp.crt_b = dev_upload(dev_allocs_, img, &table_bytes_);
+            b.dp.crt_nrows = nr;
+            b.dp.crt_kbytes = kb;
+            b.mode = (j0 == 0 && v0 == 0) ? CRT_PARTIAL_FIRST : CRT_PARTIAL_ADD;
+            b.limb0 = v0 / 4;
+            b.add_s = v0 == 0;
+            b.smem = crt_tc_smem(b.dp, true);
+            crt_blocks_.push_back(b);
+        }
+    }
+    return true;
+}
+
+void Engine::reserve_crt_partials(size_t coeffs) {
+    if (!crt_blocked_ || coeffs <= partial_coeffs_) return;
+    if (d_zp_) cudaFree(d_zp_);
+    if (d_sp_) cudaFree(d_sp_);
+    d_zp_ = nullptr;
+    d_sp_ = nullptr;
+    partial_coeffs_ = 0;
+    cuda_check(cudaMalloc(&d_zp_, coeffs * crt_zl(plan_.L) * 4), "cudaMalloc CRT partials");
+    cuda_check(cudaMalloc(&d_sp_, coeffs * 4), "cudaMalloc CRT partials");
+    partial_coeffs_ = coeffs;
+}
+
+int Engine::kernel_launches_per_group() const {
+    const int dec = dec_tc_ ? (int)dec_blocks_.size() : 1;
+    const int crt = crt_blocked_ ? (int)crt_blocks_.size() + 1 : 1;
+    return 2 * dec + crt + (plan_.w1 > 0 ? 5 : 3);
+}
 
 ChunkMap Engine::chunk_map(Chunk ch) const {
     ChunkMap m;
@@ -481,12 +596,15 @@ ChunkMap Engine::chunk_map(Chunk ch) const {
 // ---------------------------------------------------------------------------------------
 void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s) const {
     const uint32_t npos = plan_.nrows * ch.cw;
-    if (form_ == GEMM_TENSOR) {
+    if (dec_tc_) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         const int bulk = ((uintptr_t)src % 16 == 0) && ((size_t)npos * plan_.L * 4) % 16 == 0;
-        k_rns_tc<<<grid, RNS_TC_THREADS, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, nb, R, bulk);
-        cuda_check(cudaGetLastError(), "launch k_rns_tc");
+        for (const DecBlock& b : dec_blocks_) {
+            k_rns_tc<<<grid, RNS_TC_THREADS, b.smem, s>>>(b.dp, src, chunk_map(ch), npos, nb,
+                                                            R + (size_t)b.j0 * plan_.N, bulk);
+            cuda_check(cudaGetLastError(), "launch k_rns_tc");
+        }
     } else {
         dim3 grid((npos + DEC_TM - 1) / DEC_TM, 1, nb);
         k_rns_plain<<<grid, 256, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, R, dec_tab_smem_ ? 1 : 0);
@@ -510,13 +628,30 @@ void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t n
     cuda_check(cudaGetLastError(), fused ? "launch k_ntt_rows<fused>" : "launch k_ntt_rows<forward>");
 }
 
-void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s) const {
+void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff) const {
     const uint32_t npos = plan_.nrows * ch.cw;
-    if (form_ == GEMM_TENSOR) {
+    if (crt_tc_) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
-        k_crt_tc<<<grid, CRT_TC_THREADS, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out);
+        const CrtPartial full{nullptr, nullptr, CRT_FULL, 0, 0};
+        k_crt_tc<<<grid, CRT_TC_THREADS, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out, full);
         cuda_check(cudaGetLastError(), "launch k_crt_tc");
+    } else if (crt_blocked_) {
+        const size_t coeffs = (size_t)npos * nb;
+        if (poff + coeffs > partial_coeffs_) throw Unsupported("blocked CRT: partial buffers reserved for fewer coefficients");
+        uint32_t* zp = d_zp_ + poff * crt_zl(plan_.L);
+        float* sp = d_sp_ + poff;
+        const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
+        const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
+        for (const CrtBlock& b : crt_blocks_) {
+            const CrtPartial part{zp, sp, b.mode, b.limb0, b.add_s};
+            k_crt_tc<<<grid, CRT_TC_THREADS, b.smem, s>>>(b.dp, R + (size_t)b.j0 * plan_.N, chunk_map(ch), npos, nb,
+                                                            out, part);
+            cuda_check(cudaGetLastError(), "launch k_crt_tc (block)");
+        }
+        const size_t fsmem = (size_t)TC_M * crt_zstride(plan_.L) * 4;
+        k_crt_finish<<<(unsigned)((coeffs + TC_M - 1) / TC_M), TC_M, fsmem, s>>>(dp_, zp, sp, (uint32_t)coeffs, out);
+        cuda_check(cudaGetLastError(), "launch k_crt_finish");
     } else {
         dim3 grid((npos + CRT_TM - 1) / CRT_TM, 1, nb);
         k_crt_plain<<<grid, 128, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, out);
@@ -714,7 +849,8 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         cudaStream_t sc = s_comp_[oc % 3];
         if (oc % 3 != 0) cuda_check(cudaStreamWaitEvent(sc, ev_fused_, 0), "wait");
         launch_cols(true, d_rb_, ch, 1, sc);
-        launch_crt(d_rb_, ch, 1, d_out_ + off, sc);
+        // output chunks run on three streams: each gets its own region of the partial buffers
+        launch_crt(d_rb_, ch, 1, d_out_ + off, sc, (size_t)ch.col0 * nrows);
         cuda_check(cudaEventRecord(ev_crt_[oc], sc), "record");
         mark("crt" + std::to_string(oc), sc);
         cuda_check(cudaStreamWaitEvent(s_d2h_, ev_crt_[oc], 0), "wait");

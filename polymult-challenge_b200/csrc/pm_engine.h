@@ -62,7 +62,7 @@ class HostPool {
     std::condition_variable cv_;
 };
 
-enum GemmForm : int { GEMM_AUTO = 0, GEMM_PLAIN = 1, GEMM_TENSOR = 2 };
+enum GemmForm : int { GEMM_AUTO = 0, GEMM_PLAIN = 1, GEMM_TENSOR = 2, GEMM_MIXED = 3 };
 
 struct Chunk {
     uint32_t col0, cw;
@@ -98,6 +98,9 @@ class Engine {
                      float* ms_out);
     // One multiply from host (pageable) operands to a host result; synchronous.
     void run_host(const uint32_t* a, const uint32_t* b, uint32_t* c);
+    // Device memory for `coeffs` coefficients of a blocked CRT per launch (no-op otherwise);
+    // called before a CUDA-graph capture so that no allocation happens inside it.
+    void reserve(size_t coeffs) { reserve_crt_partials(coeffs); }
     // Host pipeline column-chunk schedule (powers of two: body chunks of ncols / divisor).
     void set_chunk_schedule(uint32_t in_body, uint32_t out_body);
     // Measures the candidate schedules on run_host and keeps the fastest; median ms.
@@ -124,9 +127,26 @@ class Engine {
     void launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s) const;
     void launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s,
                      const uint32_t* ra_sel = nullptr) const;
-    void launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s) const;
+    // `poff`: first coefficient of this launch's region of the blocked CRT's partial buffers --
+    // launches that may run concurrently (other streams) must use disjoint regions
+    void launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff = 0) const;
 
   private:
+    struct DecBlock {
+        DevPlan dp;        // the block's view of the plan (primes j0 .. j0 + dp.K)
+        uint32_t j0 = 0;
+        size_t smem = 0;
+    };
+    bool make_dec_blocks();
+    // (prime block, result-byte block) launches of a CRT too large for one tile
+    struct CrtBlock {
+        DevPlan dp;
+        uint32_t j0 = 0;
+        int mode = 0, limb0 = 0, add_s = 0;
+        size_t smem = 0;
+    };
+    bool make_crt_blocks();
+    void reserve_crt_partials(size_t coeffs);
     void upload_tables();
     void setup_launch_shapes();
     void ensure_scratch(uint32_t group);
@@ -137,6 +157,13 @@ class Engine {
     DevPlan dp_{};
     int device_ = 0;
     int form_ = GEMM_PLAIN;
+    bool dec_tc_ = false, crt_tc_ = false;  // which contractions run on the tensor cores
+    bool crt_blocked_ = false;              // the tensor-core CRT runs in blocks (K > one tile)
+    std::vector<DecBlock> dec_blocks_;
+    std::vector<CrtBlock> crt_blocks_;
+    uint32_t* d_zp_ = nullptr;              // blocked CRT: partial integers [coefficients][L + 3]
+    float* d_sp_ = nullptr;                 // blocked CRT: partial sums [coefficients]
+    size_t partial_coeffs_ = 0;
     int num_sms_ = 148;
     size_t smem_optin_ = 227 * 1024;
     std::vector<void*> dev_allocs_;

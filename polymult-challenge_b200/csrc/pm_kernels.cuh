@@ -40,11 +40,24 @@ size_t crt_plain_smem(const DevPlan& P);
 constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
 __global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R,
                          int use_bulk);
-__global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out);
+// A CRT over more primes than one tile holds runs as a sequence of k_crt_tc launches over
+// (prime block, result-byte block) pairs that accumulate exact per-coefficient partial integers
+// (zl = L + 3 limbs each) and partial sums of y_j / p_j, then k_crt_finish.
+enum : int { CRT_FULL = 0, CRT_PARTIAL_FIRST = 1, CRT_PARTIAL_ADD = 2 };
+struct CrtPartial {
+    uint32_t* zp;  // [coefficients][L + 3] partial integers (coefficient = batch * npos + position)
+    float* sp;     // [coefficients] partial sums of y_j / p_j
+    int mode;      // CRT_FULL: the whole CRT, result to `out`
+    int limb0;     // the block's first result byte / 4
+    int add_s;     // whether this launch adds its sum of y_j / p_j (once per prime block)
+};
+__global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
+                         CrtPartial part);
+__global__ void k_crt_finish(DevPlan P, const uint32_t* zp, const float* sp, uint32_t total, uint32_t* out);
 constexpr int RNS_TC_THREADS = 640;  // 4 loader warps + 16 epilogue warps (4 lane quarters x 2 prime halves x 2 column sets)
 constexpr int CRT_TC_THREADS = 512;  // 256 producers + 256 epilogue threads, two per coefficient each
 size_t rns_tc_smem(const DevPlan& P);
-size_t crt_tc_smem(const DevPlan& P);
+size_t crt_tc_smem(const DevPlan& P, bool partial = false);
 // TMEM columns to allocate: a power of two >= max(32, n)
 __host__ __device__ inline uint32_t tmem_cols_for(int n) {
     uint32_t c = 32;

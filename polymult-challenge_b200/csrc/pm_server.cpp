@@ -58,6 +58,7 @@ Server::Server(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const uint
             return static_cast<uint32_t*>(p);
         };
         resident_ = dalloc((size_t)nres_ * rw);
+        eng_->reserve((size_t)ns * cap_ * P.N);  // a blocked CRT's partials: one region per slot
         slots_.resize(ns);
         for (Slot& s : slots_) {
             cuda_check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream");
@@ -136,7 +137,7 @@ void Server::launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint
     eng_->launch_cols(false, s.res, all, nb, s.stream);
     eng_->launch_rows(true, s.res, resident_, nb, s.stream, s.sel_d);
     eng_->launch_cols(true, s.res, all, nb, s.stream);
-    eng_->launch_crt(s.res, all, nb, s.out, s.stream);
+    eng_->launch_crt(s.res, all, nb, s.out, s.stream, (size_t)(&s - slots_.data()) * cap_ * P.N);
     for (uint32_t i = 0; i < nb; ++i)
         cuda_check(cudaMemcpyAsync(c[s.reqs[i]], s.out + i * cw, cw * 4, cudaMemcpyDeviceToHost, s.stream),
                    "result D2H");

@@ -27,7 +27,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libpolymult_b200.so")
 HEADER = os.path.join(HERE, "..", "include", "polymult_b200.h")
 
 PM_OK, PM_ERR_INVALID, PM_ERR_CUDA, PM_ERR_DEVICE, PM_ERR_UNSUPPORTED, PM_ERR_INTERNAL = range(6)
-GEMM_FORMS = {"auto": 0, "plain": 1, "tensor": 2}
+GEMM_FORMS = {"auto": 0, "plain": 1, "tensor": 2, "mixed": 3}
 GEMM_NAMES = {v: k for k, v in GEMM_FORMS.items()}
 STAGES = ("dec_a", "cols_a", "rows_a", "dec_b", "cols_b", "rows_fused", "cols_inv", "crt")
 

@@ -156,3 +156,41 @@ def test_tuned_pipeline_still_bit_exact():
             a, b, _ = regen_case(pt, case)
             assert sha(m.multiply(a, b)) == case["c_sha256"], (case["s"], case["mode"])
         m.sync()
+
+
+def test_wide_points_on_tensor_cores_in_blocks():
+    """Above K = 128 primes (W beyond about 1900 bits) one tcgen05 tile no longer holds every
+    prime: the decomposition runs in prime blocks and the CRT in (prime block, result-byte block)
+    launches that accumulate exact partial integers, finished by one CUDA-core pass.  Bit-exact
+    on the reference's W = 4000 golden point and, against the C oracle and the plain form, on a
+    W = 3000 point of the batch grid."""
+    import workload
+    pt = next(p for p in POINTS if p["W"] == 4000)
+    with _multiplier(pt, "auto") as m:
+        assert m.info()["gemm"] in ("tensor", "mixed")
+        for case in pt["cases"]:
+            a, b, _ = regen_case(pt, case)
+            assert sha(m.multiply(a, b)) == case["c_sha256"], (case["s"], case["mode"])
+        m.sync()
+    torch = _torch()
+    import polymult
+    N, W = 4096, 3000
+    L = (W + 31) // 32
+    q = workload.spec_prime(N, W)
+    ops = workload.uniform_operands(N, W, q, 6, seed=17)
+    da = torch.from_numpy(np.ascontiguousarray(ops[:3]).view(np.int32)).cuda()
+    db = torch.from_numpy(np.ascontiguousarray(ops[3:]).view(np.int32)).cuda()
+    outs = {}
+    for gemm in ("auto", "plain"):
+        with polymult.Multiplier(N, W, workload.limbs(q, L), gemm=gemm) as m:
+            outs[gemm] = m.info()["gemm"]
+            dc = torch.zeros_like(da)
+            m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), 3, torch.cuda.current_stream().cuda_stream)
+            m.sync()
+            outs[gemm + "_c"] = dc.cpu().numpy().view(np.uint32)
+            host = m.multiply(ops[0], ops[3])  # the chunked host pipeline as well
+            assert np.array_equal(host, outs[gemm + "_c"][0])
+    assert outs["auto"] == "tensor" and outs["plain"] == "plain"
+    assert np.array_equal(outs["auto_c"], outs["plain_c"])
+    for i in range(3):
+        assert np.array_equal(outs["auto_c"][i], c_oracle_mul(N, W, q, ops[i], ops[3 + i])), i

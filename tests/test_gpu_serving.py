@@ -55,7 +55,8 @@ def _serve(srv, reqs, sel, t_arrive):
     return np.array(c), lat, st
 
 
-@pytest.mark.parametrize("N,W,nres,nreq", [(4096, 256, 3, 40), (2048, 868, 8, 24), (65536, 1747, 8, 12)])
+@pytest.mark.parametrize("N,W,nres,nreq", [(4096, 256, 3, 40), (2048, 868, 8, 24), (65536, 1747, 8, 12),
+                                            (4096, 3000, 4, 16)])
 def test_mixed_requests_equal_alone(N, W, nres, nreq):
     torch = _torch()
     import polymult
