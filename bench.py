@@ -538,12 +538,14 @@ def run_ours(args):
            "chunk_schedule": pipe,
            "p50_over_floor": round(lat_ms[len(lat_ms) // 2] / floor_ms, 3)}
 
+    # the uneven-batch and serving legs run on rank 0 only (no collectives; with N > 1 the
+    # other ranks are done after the end-to-end leg): they describe one GPU's batch and server
     batched = None
-    if not args.no_batched:
+    if not args.no_batched and rank == 0:
         batched = run_batched(torch, args, local)
 
     serving = None
-    if not args.no_serving:
+    if not args.no_serving and rank == 0:
         serving = run_serving(args, local)
 
     cpu = None
