@@ -86,6 +86,18 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+// 32 TMEM lanes (this warp's) x 16 consecutive 32-bit columns, without waiting: the registers
+// are valid after tmem_wait_ld().  Issuing several before one wait overlaps their latency.
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // 32 TMEM lanes (this warp's) x 16 consecutive 32-bit columns.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
@@ -342,17 +354,26 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
             const int j0 = half ? KH : 0;
             const int cols = half ? n1 : n0;
             const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
-            for (int c16 = sub; c16 < cols / 16 && got; c16 += 2) {
-                uint32_t r[16];
-                tmem_ld16(tcol + (uint32_t)(16 * c16), r);
+            // this thread's 16-column chunks c16 = sub, sub + 2, ...: two TMEM loads in flight per wait
+            const int nch = cols / 16;
+            for (int c16 = sub; c16 < nch && got; c16 += 4) {
+                uint32_t r[2][16];
+                const bool two = c16 + 2 < nch;
+                tmem_ld16_async(tcol + (uint32_t)(16 * c16), r[0]);
+                if (two) tmem_ld16_async(tcol + (uint32_t)(16 * (c16 + 2)), r[1]);
+                tmem_wait_ld();
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int j = j0 + 4 * c16 + q;
-                    if (j < P.K && m < cnt) {
-                        const uint64_t x = (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
-                                           ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24);
-                        const uint32_t p = __ldg(P.p + j);
-                        Rb[(size_t)j * P.N] = red_once(redc64(x, p, __ldg(P.pinv + j)), p);
+                for (int u = 0; u < 2; ++u) {
+                    if (u == 1 && !two) break;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int j = j0 + 4 * (c16 + 2 * u) + q;
+                        if (j < P.K && m < cnt) {
+                            const uint64_t x = (uint64_t)r[u][4 * q] + ((uint64_t)r[u][4 * q + 1] << 8) +
+                                               ((uint64_t)r[u][4 * q + 2] << 16) + ((uint64_t)r[u][4 * q + 3] << 24);
+                            const uint32_t p = __ldg(P.p + j);
+                            Rb[(size_t)j * P.N] = red_once(redc64(x, p, __ldg(P.pinv + j)), p);
+                        }
                     }
                 }
             }
@@ -556,19 +577,29 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             uint64_t carry = 0;
             const int c0 = hf ? lh / 4 : 0, c1 = hf ? nl / 4 : lh / 4;
             int l = 4 * c0;
-            for (int c16 = c0; c16 < c1; ++c16) {
-                uint32_t r[16];
-                if (got) tmem_ld16(tacc + (uint32_t)(16 * c16), r);
-                else
+            for (int c16 = c0; c16 < c1; c16 += 2) {
+                // two TMEM loads in flight per wait
+                uint32_t r[2][16];
+                const bool two = c16 + 1 < c1;
+                if (got) {
+                    tmem_ld16_async(tacc + (uint32_t)(16 * c16), r[0]);
+                    if (two) tmem_ld16_async(tacc + (uint32_t)(16 * (c16 + 1)), r[1]);
+                    tmem_wait_ld();
+                } else {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) r[k] = 0u;
+                    for (int k = 0; k < 16; ++k) r[0][k] = r[1][k] = 0u;
+                }
 #pragma unroll
-                for (int q = 0; q < 4; ++q, ++l) {
-                    const uint64_t t = carry + (uint64_t)r[4 * q] + ((uint64_t)r[4 * q + 1] << 8) +
-                                       ((uint64_t)r[4 * q + 2] << 16) + ((uint64_t)r[4 * q + 3] << 24) +
-                                       (l < L ? (uint64_t)(uint32_t)v * __ldg(T1 + l) : 0ull);
-                    if (l < zl) z[l] = (uint32_t)t;
-                    carry = t >> 32;
+                for (int u = 0; u < 2; ++u) {
+                    if (u == 1 && !two) break;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q, ++l) {
+                        const uint64_t t = carry + (uint64_t)r[u][4 * q] + ((uint64_t)r[u][4 * q + 1] << 8) +
+                                           ((uint64_t)r[u][4 * q + 2] << 16) + ((uint64_t)r[u][4 * q + 3] << 24) +
+                                           (l < L ? (uint64_t)(uint32_t)v * __ldg(T1 + l) : 0ull);
+                        if (l < zl) z[l] = (uint32_t)t;
+                        carry = t >> 32;
+                    }
                 }
             }
             if (hf) {
@@ -623,23 +654,20 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 }
                 continue;
             }
-            // coalesced store of the tile's cnt x L limbs (contiguous in the output)
+            // coalesced store of the tile's cnt x L limbs (contiguous in the output); element w =
+            // row mm, limb col is tracked incrementally (w advances by 256 = qL rows + rL limbs)
             uint32_t* o = out + ((size_t)bt * npos + pos0) * L;
             const int tot = cnt * L;
-            int w = et;
-            for (; w + 3 * CRT_EPI_THREADS < tot; w += 4 * CRT_EPI_THREADS) {
-                uint32_t v4[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int ww = w + u * CRT_EPI_THREADS, mm = ww / L;
-                    v4[u] = S.z[(size_t)mm * zs + (ww - mm * L)];
+            const int qL = CRT_EPI_THREADS / L, rL = CRT_EPI_THREADS - qL * L;
+            int mm = et / L, col = et - mm * L;
+            for (int w = et; w < tot; w += CRT_EPI_THREADS) {
+                o[w] = S.z[(size_t)mm * zs + col];
+                mm += qL;
+                col += rL;
+                if (col >= L) {
+                    col -= L;
+                    ++mm;
                 }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) o[w + u * CRT_EPI_THREADS] = v4[u];
-            }
-            for (; w < tot; w += CRT_EPI_THREADS) {
-                const int mm = w / L;
-                o[w] = S.z[(size_t)mm * zs + (w - mm * L)];
             }
         }
     }
