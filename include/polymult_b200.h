@@ -202,12 +202,19 @@ typedef struct pm_pipeline_info {
     double tuned_ms;                /* median pm_run time of the chosen schedule (0: not tuned) */
 } pm_pipeline_info;
 
+/* pm_run keeps two schedules: one for calls whose buffers it stages through its host threads
+ * (pageable memory; the reference's case) and one for calls whose a, b and c are all
+ * page-locked (cudaHostAlloc / cudaHostRegister), which it copies chunk by chunk with strided
+ * DMA copies and no host staging.  `flags` selects the second with PM_PIPELINE_PINNED. */
+#define PM_PIPELINE_PINNED 1
+
 /* No reference counterpart: the autotuner of the host pipeline.  Runs `reps` pm_run calls (plus
- * a warm-up) for every schedule with body divisors in {4, 8, 16} x {4, 8, 16}, keeps the one
- * with the lowest median wall time, and describes it in *out.  Synchronous; about 10 x (reps + 1)
+ * a warm-up) for every schedule with body divisors in {4, 8, 16} x {4, 8, 16} on pageable (or,
+ * with PM_PIPELINE_PINNED, page-locked) timing buffers, keeps the one with the lowest median wall
+ * time for that kind of call, and describes it in *out.  Synchronous; about 10 x (reps + 1)
  * calls. */
-int pm_tune_pipeline(pm_context* ctx, int reps, pm_pipeline_info* out);
-int pm_get_pipeline(const pm_context* ctx, pm_pipeline_info* out);
+int pm_tune_pipeline(pm_context* ctx, int reps, int flags, pm_pipeline_info* out);
+int pm_get_pipeline(const pm_context* ctx, int flags, pm_pipeline_info* out);
 
 /* Waits for the context's device work and returns PM_ERR_DEVICE if a device-side check
  * failed since the last call. */

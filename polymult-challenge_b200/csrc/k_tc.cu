@@ -207,7 +207,7 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
 // So tile i's epilogue (the long phase) overlaps tile i+1's copy, relayout and MMAs.  Bounded
 // waits with a shared abort flag as in the CRT kernel.
 // smem: [B image][A tile][raw ring 2 x 128*L words][bars: B, raw 2, mma_done 2, acc_empty 2]
-//       [slot][abort]
+//       [slot][abort][{p, p^-1 mod 2^32} x KP]
 // ----------------------------------------------------------------------------------------
 constexpr int DEC_LOAD_THREADS = 128;
 constexpr int DEC_EPI_THREADS = 512;
@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
     uint64_t *bar_b = bars, *bar_raw = bars + 1, *mma_done = bars + 3, *acc_empty = bars + 5;
     uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 7);
     volatile int* abort_f = reinterpret_cast<volatile int*>(slot + 1);
+    uint2* pc_s = reinterpret_cast<uint2*>(slot + 2);  // [KP] {p, p^-1 mod 2^32}
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t ncols = tmem_cols_for((int)col1 + n1);
     const int nhalves = n1 > 0 ? 2 : 1;
@@ -260,6 +261,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                 }
             }
     }
+    for (int j = threadIdx.x; j < P.KP; j += blockDim.x) pc_s[j] = make_uint2(P.p[j], P.pinv[j]);
     if (warp == 0) tmem_alloc(slot, ncols);
     tc_fence_before();
     __syncthreads();
@@ -335,6 +337,9 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         }
     } else {
         // ---------------- epilogue ----------------
+        // every byte-column sum is < 255 * 255 * kb; with kb <= 256 the two-byte partial sums
+        // r0 + r1 2^8 and r2 + r3 2^8 stay below 2^32 and x is formed in 32-bit halves
+        const bool small_k = kb <= 256;
         const int we = warp - DEC_LOAD_THREADS / 32;
         const int half = (we >> 2) & 1, sub = we >> 3, m = (warp & 3) * 32 + lane;
         const bool active = half < nhalves;
@@ -354,26 +359,46 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
             const int j0 = half ? KH : 0;
             const int cols = half ? n1 : n0;
             const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
-            // this thread's 16-column chunks c16 = sub, sub + 2, ...: two TMEM loads in flight per wait
+            // this thread's 16-column chunks c16 = sub, sub + 2, ...: two TMEM loads in flight per
+            // wait, the chunks' prime constants read from shared memory while they are in flight
             const int nch = cols / 16;
+            const bool st = m < cnt;
             for (int c16 = sub; c16 < nch && got; c16 += 4) {
                 uint32_t r[2][16];
+                uint2 pc[2][4];
                 const bool two = c16 + 2 < nch;
+                // (the second chunk's constants only if it exists: past the last chunk of half 1
+                // the index would leave the table)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    pc[0][q] = pc_s[j0 + 4 * c16 + q];
+                    pc[1][q] = two ? pc_s[j0 + 4 * (c16 + 2) + q] : make_uint2(0u, 0u);
+                }
                 tmem_ld16_async(tcol + (uint32_t)(16 * c16), r[0]);
                 if (two) tmem_ld16_async(tcol + (uint32_t)(16 * (c16 + 2)), r[1]);
                 tmem_wait_ld();
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     if (u == 1 && !two) break;
+                    const int jb = j0 + 4 * (c16 + 2 * u);
+                    uint32_t* out = Rb + (size_t)jb * P.N;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const int j = j0 + 4 * (c16 + 2 * u) + q;
-                        if (j < P.K && m < cnt) {
-                            const uint64_t x = (uint64_t)r[u][4 * q] + ((uint64_t)r[u][4 * q + 1] << 8) +
-                                               ((uint64_t)r[u][4 * q + 2] << 16) + ((uint64_t)r[u][4 * q + 3] << 24);
-                            const uint32_t p = __ldg(P.p + j);
-                            Rb[(size_t)j * P.N] = red_once(redc64(x, p, __ldg(P.pinv + j)), p);
+                        const uint32_t p = pc[u][q].x, pinv = pc[u][q].y;
+                        const uint32_t* rq = &r[u][4 * q];
+                        uint32_t y;
+                        if (small_k) {
+                            // x = t0 + t1 2^16 with t0 = r0 + r1 2^8, t1 = r2 + r3 2^8 < 2^32
+                            const uint32_t t0 = rq[0] + (rq[1] << 8), t1 = rq[2] + (rq[3] << 8);
+                            const uint32_t lo = t0 + (t1 << 16);
+                            const uint32_t hi = (t1 >> 16) + (lo < t0 ? 1u : 0u);
+                            y = red_once(hi - __umulhi(lo * pinv, p) + p, p);
+                        } else {
+                            const uint64_t x = (uint64_t)rq[0] + ((uint64_t)rq[1] << 8) + ((uint64_t)rq[2] << 16) +
+                                               ((uint64_t)rq[3] << 24);
+                            y = red_once(redc64(x, p, pinv), p);
                         }
+                        if (st && jb + q < P.K) out[(size_t)q * P.N] = y;
                     }
                 }
             }
@@ -468,27 +493,40 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
 
     if (threadIdx.x < CRT_PROD_THREADS) {
         // ---------------- producers ----------------
+        // thread (m, h): position m of the tile, groups [g0, g0 + ng) of 4 primes (half h of
+        // the G = KP / 4 groups; the padding primes K..KP-1 have zero constants, so they add
+        // nothing to A's product with the zero B columns nor to the partial sums)
         const int m = threadIdx.x & (TC_M - 1), h = threadIdx.x >> 7;
-        const int kgroups = kb / 16;
-        const int gh = (kgroups + 1) / 2;
-        const int g0 = h ? gh : 0, ng = (h ? kgroups : gh) - g0;
+        const int G = KP / 4;
+        const int gh = (G + 1) / 2;
+        const int g0 = h ? gh : 0, ng = (h ? G : gh) - g0;
+        const size_t N = P.N;
+        unsigned char* arow = S.a + (size_t)(m >> 3) * sbo + (m & 7) * 16;
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(1, CRT_PROD_THREADS, *S.abort != 0)) break;
             const int b = (int)(i & 1);
             const uint32_t bt = tile / tiles_per_batch;
             const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
-            const bool valid = (uint32_t)m < npos - pos0;
-            const uint32_t* Rm = R + (size_t)bt * P.Kr * P.N + (valid ? chunk_pos_to_n(P, C, pos0 + m) : 0u);
+            // positions past the end of the batch repeat the tile's first one: their A rows and
+            // partial sums only feed accumulator rows the epilogue does not store
+            const uint32_t pm = (uint32_t)m < npos - pos0 ? pos0 + m : pos0;
+            const uint32_t* rp = R + (size_t)bt * P.Kr * N + chunk_pos_to_n(P, C, pm) + (size_t)(4 * g0) * N;
             // residues in batches of CRT_BATCH_GROUPS groups (4 primes each), the next batch's
-            // loads in flight while this batch is converted: up to 2 x 16 loads per thread
+            // loads in flight while this batch is converted: up to 2 x 12 loads per thread
             float s4[4] = {0.f, 0.f, 0.f, 0.f};
             uint32_t xa[4 * CRT_BATCH_GROUPS], xb[4 * CRT_BATCH_GROUPS];
             auto load_batch = [&](uint32_t(&x)[4 * CRT_BATCH_GROUPS], int bat) {
+                const uint32_t* q = rp + (size_t)(4 * CRT_BATCH_GROUPS * bat) * N;
+                // primes left from the batch's first (>= 1: its first group is this half's);
+                // slots past them re-read the last one and are not converted
+                const int left = K - 4 * (g0 + CRT_BATCH_GROUPS * bat);
+                if (left >= 4 * CRT_BATCH_GROUPS) {
 #pragma unroll
-                for (int u = 0; u < 4 * CRT_BATCH_GROUPS; ++u) {
-                    const int gg = bat * CRT_BATCH_GROUPS + u / 4, j = 4 * (g0 + gg) + (u & 3);
-                    x[u] = (gg < ng && j < K && valid) ? __ldg(Rm + (size_t)j * P.N) : 0u;
+                    for (int u = 0; u < 4 * CRT_BATCH_GROUPS; ++u) x[u] = __ldg(q + (size_t)u * N);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 4 * CRT_BATCH_GROUPS; ++u) x[u] = __ldg(q + (size_t)min(u, left - 1) * N);
                 }
             };
             auto convert_batch = [&](const uint32_t(&x)[4 * CRT_BATCH_GROUPS], int bat) {
@@ -496,19 +534,15 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 for (int gl = 0; gl < CRT_BATCH_GROUPS; ++gl) {
                     const int gg = bat * CRT_BATCH_GROUPS + gl;
                     if (gg >= ng) break;
+                    const int g = g0 + gg;
                     uint32_t yy[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const int j = 4 * (g0 + gg) + q;
-                        yy[q] = 0u;
-                        if (j < K) {
-                            const uint4 c = S.cst[j];
-                            yy[q] = red_once(mul_ms(x[4 * gl + q], c.y, c.z, c.x), c.x);
-                            s4[q] = fmaf((float)yy[q], __uint_as_float(c.w), s4[q]);
-                        }
+                        const uint4 c = S.cst[4 * g + q];
+                        yy[q] = red_once(mul_ms(x[4 * gl + q], c.y, c.z, c.x), c.x);
+                        s4[q] = fmaf((float)yy[q], __uint_as_float(c.w), s4[q]);
                     }
-                    *reinterpret_cast<uint4*>(S.a + (size_t)(m >> 3) * sbo + (size_t)(g0 + gg) * 128 + (m & 7) * 16) =
-                        make_uint4(yy[0], yy[1], yy[2], yy[3]);
+                    *reinterpret_cast<uint4*>(arow + (size_t)g * 128) = make_uint4(yy[0], yy[1], yy[2], yy[3]);
                 }
             };
             const int nbat = (ng + CRT_BATCH_GROUPS - 1) / CRT_BATCH_GROUPS;
@@ -683,7 +717,8 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
 }
 
 size_t rns_tc_smem(const DevPlan& P) {
-    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + 2 * (size_t)TC_M * P.L * 4 + 7 * 8 + 16;
+    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + 2 * (size_t)TC_M * P.L * 4 + 7 * 8 + 8 +
+           (size_t)P.KP * 8;
 }
 
 size_t crt_tc_smem(const DevPlan& P, bool partial) {

@@ -123,27 +123,31 @@ int pm_get_info(const pm_context* ctx, pm_info* out) {
     return PM_OK;
 }
 
-static void fill_pipeline(const pm::Engine& e, double ms, pm_pipeline_info* out) {
+static void fill_pipeline(const pm::Engine& e, int kind, double ms, pm_pipeline_info* out) {
     std::memset(out, 0, sizeof *out);
-    out->in_chunks = (int32_t)e.in_chunks().size();
-    out->out_chunks = (int32_t)e.out_chunks().size();
-    out->in_body = (int32_t)e.in_body();
-    out->out_body = (int32_t)e.out_body();
+    out->in_chunks = (int32_t)e.in_chunks(kind).size();
+    out->out_chunks = (int32_t)e.out_chunks(kind).size();
+    out->in_body = (int32_t)e.in_body(kind);
+    out->out_body = (int32_t)e.out_body(kind);
     out->tuned_ms = ms;
 }
 
-int pm_tune_pipeline(pm_context* ctx, int reps, pm_pipeline_info* out) {
+int pm_tune_pipeline(pm_context* ctx, int reps, int flags, pm_pipeline_info* out) {
     if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    if (flags & ~PM_PIPELINE_PINNED) return fail(PM_ERR_INVALID, "unknown pipeline flags");
+    const int kind = (flags & PM_PIPELINE_PINNED) ? 1 : 0;
     return guarded([&] {
-        const double ms = ctx->engine->tune_host_pipeline(reps);
-        ctx->tuned_ms = ms;
-        if (out) fill_pipeline(*ctx->engine, ms, out);
+        const double ms = ctx->engine->tune_host_pipeline(reps, kind);
+        ctx->tuned_ms[kind] = ms;
+        if (out) fill_pipeline(*ctx->engine, kind, ms, out);
     });
 }
 
-int pm_get_pipeline(const pm_context* ctx, pm_pipeline_info* out) {
+int pm_get_pipeline(const pm_context* ctx, int flags, pm_pipeline_info* out) {
     if (!ctx || !ctx->engine || !out) return fail(PM_ERR_INVALID, "null argument");
-    fill_pipeline(*ctx->engine, ctx->tuned_ms, out);
+    if (flags & ~PM_PIPELINE_PINNED) return fail(PM_ERR_INVALID, "unknown pipeline flags");
+    const int kind = (flags & PM_PIPELINE_PINNED) ? 1 : 0;
+    fill_pipeline(*ctx->engine, kind, ctx->tuned_ms[kind], out);
     return PM_OK;
 }
 

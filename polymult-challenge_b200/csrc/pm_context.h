@@ -7,7 +7,7 @@
 
 struct pm_context {
     pm::Engine* engine;
-    double tuned_ms = 0.0;  // median pm_run of the schedule pm_tune_pipeline chose
+    double tuned_ms[2] = {0.0, 0.0};  // median pm_run of the schedule pm_tune_pipeline chose, per kind
 };
 
 struct pm_batch {

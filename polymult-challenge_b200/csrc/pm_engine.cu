@@ -395,63 +395,104 @@ void Engine::ensure_scratch(uint32_t group) {
     group_ = group;
 }
 
-// Column-chunk schedule of the host pipeline: input chunks of ncols / in_body columns after
-// narrow head chunks (1/32, 1/32, 1/16), output chunks of ncols / out_body columns between
-// narrow head and tail chunks (1/64, 1/32 ... 1/32, 1/64), so that the pipeline fills and
-// drains sooner; events sized to match.
-void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body) {
+// Column-chunk schedule of the host pipeline.  Staged calls (kind 0): input chunks of
+// ncols / in_body columns after narrow head chunks (1/32, 1/32, 1/16), output chunks of
+// ncols / out_body columns between narrow head and tail chunks (1/64, 1/32 ... 1/32, 1/64),
+// so that the host staging starts and the host scatter ends sooner.  Direct-copy calls
+// (kind 1): b in chunks of ncols / in_body (a moves whole), output in chunks of
+// ncols / out_body, no narrow heads or tails: nothing on the host precedes an H2D or follows
+// a D2H, the first output chunk's latency (inverse column pass + CRT, ~30 us at N = 65536)
+// hardly depends on its width, and each copy costs a few microseconds of DMA set-up.  Events
+// sized for the longer schedule.
+void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind) {
     if (in_body == 0 || out_body == 0 || (in_body & (in_body - 1)) || (out_body & (out_body - 1)))
         throw InvalidPoint("chunk divisors must be powers of two");
+    if (kind != 0 && kind != 1) throw InvalidPoint("pipeline kind must be 0 (staged) or 1 (direct)");
     const uint32_t nc = plan_.ncols;
-    cin_ = make_chunks(nc, {32, 32, 16}, in_body, {});
-    cout_ = make_chunks(nc, {64, 32}, out_body, {32, 64});
-    in_body_ = in_body;
-    out_body_ = out_body;
+    if (kind == 0) {
+        cin_[kind] = make_chunks(nc, {32, 32, 16}, in_body, {});
+        cout_[kind] = make_chunks(nc, {64, 32}, out_body, {32, 64});
+    } else {
+        cin_[kind] = make_chunks(nc, {}, in_body, {});
+        cout_[kind] = make_chunks(nc, {}, out_body, {});
+    }
+    in_body_[kind] = in_body;
+    out_body_[kind] = out_body;
+    // input items: both operands' chunks (kind 0), or a whole plus b's chunks (kind 1)
+    const size_t nin = std::max(2 * cin_[0].size(), 1 + cin_[1].size());
+    const size_t nco = std::max(cout_[0].size(), cout_[1].size());
     auto mk = [](std::vector<cudaEvent_t>& v, size_t n, unsigned flags) {
+        if (v.size() == n) return;
         for (auto e : v) cudaEventDestroy(e);
         v.assign(n, nullptr);
         for (auto& e : v) cuda_check(cudaEventCreateWithFlags(&e, flags), "event");
     };
-    mk(ev_in_, 2 * cin_.size(), cudaEventDisableTiming);
-    mk(ev_done_in_, 2 * cin_.size(), cudaEventDisableTiming);
-    mk(ev_crt_, cout_.size(), cudaEventDisableTiming);
-    mk(ev_out_, cout_.size(), cudaEventDisableTiming);
-    if (profile_) mk(trace_ev_, 8 + 2 * 2 * cin_.size() + 2 * cout_.size(), cudaEventDefault);
+    mk(ev_in_, nin, cudaEventDisableTiming);
+    mk(ev_done_in_, nin, cudaEventDisableTiming);
+    mk(ev_crt_, nco, cudaEventDisableTiming);
+    mk(ev_out_, nco, cudaEventDisableTiming);
+    if (profile_) mk(trace_ev_, 8 + 2 * nin + 2 * nco, cudaEventDefault);
 }
 
-// Times every (in_body, out_body) in {4, 8, 16}^2 on `reps` calls of run_host (after one
-// warm-up call each) and keeps the schedule with the lowest median; returns that median (ms).
-double Engine::tune_host_pipeline(int reps) {
+double Engine::tune_host_pipeline(int reps, int kind) {
     if (!pool_) throw Unsupported("this context has no host pipeline");
+    if (kind != 0 && kind != 1) throw InvalidPoint("pipeline kind must be 0 (staged) or 1 (direct)");
     reps = std::max(1, reps);
     // timing operand: pseudo-random limbs with the top limb of every coefficient zero, so that
-    // each coefficient is below 2^(32(L-1)) < q (the kernels' bounds assume inputs below q)
-    std::vector<uint32_t> a(plan_.coeff_words(), 0), c(plan_.coeff_words());
-    for (size_t i = 0; i < a.size(); ++i)
-        a[i] = (i % plan_.L == plan_.L - 1) ? 0u : (uint32_t)(i * 2654435761u);
-    double best = 1e30;
-    uint32_t bi = in_body_, bo = out_body_;
-    const uint32_t cand[3] = {4, 8, 16};
-    for (uint32_t ib : cand)
-        for (uint32_t ob : cand) {
-            if (ib > plan_.ncols || ob > plan_.ncols) continue;
-            set_chunk_schedule(ib, ob);
-            run_host(a.data(), a.data(), c.data());
-            std::vector<double> t;
-            for (int r = 0; r < reps; ++r) {
-                const auto t0 = std::chrono::steady_clock::now();
-                run_host(a.data(), a.data(), c.data());
-                t.push_back(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-            }
-            std::sort(t.begin(), t.end());
-            const double med = t[t.size() / 2];
-            if (med < best) {
-                best = med;
-                bi = ib;
-                bo = ob;
-            }
+    // each coefficient is below 2^(32(L-1)) < q (the kernels' bounds assume inputs below q);
+    // kind 1 times page-locked buffers (the direct-copy path)
+    const size_t words = plan_.coeff_words();
+    std::vector<uint32_t> va, vc;
+    uint32_t *a = nullptr, *c = nullptr;
+    if (kind == 1) {
+        cuda_check(cudaHostAlloc(&a, words * 4, cudaHostAllocDefault), "cudaHostAlloc");
+        if (cudaHostAlloc(&c, words * 4, cudaHostAllocDefault) != cudaSuccess) {
+            cudaFreeHost(a);
+            throw CudaError("cudaHostAlloc failed");
         }
-    set_chunk_schedule(bi, bo);
+    } else {
+        va.resize(words);
+        vc.resize(words);
+        a = va.data();
+        c = vc.data();
+    }
+    for (size_t i = 0; i < words; ++i) a[i] = (i % plan_.L == plan_.L - 1) ? 0u : (uint32_t)(i * 2654435761u);
+    double best = 1e30;
+    uint32_t bi = in_body_[kind], bo = out_body_[kind];
+    const uint32_t cand[3] = {4, 8, 16};
+    try {
+        for (uint32_t ib : cand)
+            for (uint32_t ob : cand) {
+                if (ib > plan_.ncols || ob > plan_.ncols) continue;
+                set_chunk_schedule(ib, ob, kind);
+                run_host(a, a, c);
+                std::vector<double> t;
+                for (int r = 0; r < reps; ++r) {
+                    const auto t0 = std::chrono::steady_clock::now();
+                    run_host(a, a, c);
+                    t.push_back(
+                        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+                }
+                std::sort(t.begin(), t.end());
+                const double med = t[t.size() / 2];
+                if (med < best) {
+                    best = med;
+                    bi = ib;
+                    bo = ob;
+                }
+            }
+    } catch (...) {
+        if (kind == 1) {
+            cudaFreeHost(a);
+            cudaFreeHost(c);
+        }
+        throw;
+    }
+    if (kind == 1) {
+        cudaFreeHost(a);
+        cudaFreeHost(c);
+    }
+    set_chunk_schedule(bi, bo, kind);
     return best;
 }
 
@@ -470,7 +511,8 @@ void Engine::setup_host_pipeline() {
     for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
-    set_chunk_schedule(8, 8);
+    set_chunk_schedule(8, 8, 0);
+    set_chunk_schedule(8, 8, 1);
     cuda_check(cudaEventCreateWithFlags(&ev_row_a_, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
     // 8 copying threads (7 workers + the caller) by default.  On the 16-CPU B200 hosts measured,
@@ -776,19 +818,50 @@ void Engine::throw_if_status() {
 // ---------------------------------------------------------------------------------------
 // host-operand multiply: the chunked pipeline
 // ---------------------------------------------------------------------------------------
+// True if [p, p + bytes) is page-locked host memory this device can copy from / to directly.
+static bool host_range_pinned(const void* p, size_t bytes) {
+    auto pinned = [](const void* q) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, q) != cudaSuccess) {
+            cudaGetLastError();  // an unknown pointer is not an error here
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    return bytes > 0 && pinned(p) && pinned(static_cast<const char*>(p) + bytes - 1);
+}
+
 void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
     ensure_scratch(1);
     const uint32_t nrows = plan_.nrows, ncols = plan_.ncols, L = plan_.L;
     const uint32_t* src[2] = {a, b};
-    const int na = (int)cin_.size(), nin = 2 * na;
     const uint32_t ntasks = std::min<uint32_t>(nrows, 64);
     const uint32_t rpt = (nrows + ntasks - 1) / ntasks;
+    // operands already in page-locked memory skip the host staging: each column chunk moves
+    // with one strided DMA copy (rows of cw * L words at a pitch of ncols * L words); with all
+    // three page-locked the call runs the direct-copy schedule
+    const size_t opbytes = plan_.coeff_words() * 4, pitch = (size_t)ncols * L * 4;
+    const bool direct_in[2] = {host_range_pinned(a, opbytes), host_range_pinned(b, opbytes)};
+    const bool direct_out = host_range_pinned(c, opbytes);
+    const int kind = direct_in[0] && direct_in[1] && direct_out ? 1 : 0;
+    const std::vector<Chunk>& cout = cout_[kind];
+    // input items (operand, column chunk): both operands in the schedule's input chunks; with
+    // direct copies a moves in one piece (each copy costs a few microseconds of DMA set-up, and
+    // a's transform is hidden under b's transfer anyway) and only b is chunked
+    std::vector<std::pair<int, Chunk>> items;
+    if (kind == 1) items.push_back({0, Chunk{0, ncols}});
+    else
+        for (const Chunk& ch : cin_[kind]) items.push_back({0, ch});
+    const int na = (int)items.size();
+    for (const Chunk& ch : cin_[kind]) items.push_back({1, ch});
+    const int nin = (int)items.size();
 
-    // gather input chunk i (operand i / na) into pinned memory, layout [row][col-in-chunk][limb]
+    // gather input item i into pinned memory, layout [row][col-in-chunk][limb]
     auto stage = [&](int i) {
-        const int P = i / na;
-        const Chunk ch = cin_[i % na];
+        const int P = items[i].first;
+        if (direct_in[P]) return;
+        const Chunk ch = items[i].second;
         uint32_t* dst = h_in_[P] + (size_t)ch.col0 * nrows * L;
         const size_t seg = (size_t)ch.cw * L;
         pool_->run((int)ntasks, [&](int t) {
@@ -814,11 +887,17 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     stage(0);
     t_stage0 = clk::now();
     for (int i = 0; i < nin; ++i) {
-        const int P = i / na, ci = i % na;
-        const Chunk ch = cin_[ci];
+        const int P = items[i].first;
+        const Chunk ch = items[i].second;
         const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
         cudaStream_t sc = s_comp_[i % 3];
-        cuda_check(cudaMemcpyAsync(d_in_[P] + off, h_in_[P] + off, words * 4, cudaMemcpyHostToDevice, s_h2d_), "H2D");
+        if (direct_in[P])
+            cuda_check(cudaMemcpy2DAsync(d_in_[P] + off, (size_t)ch.cw * L * 4, src[P] + (size_t)ch.col0 * L, pitch,
+                                         (size_t)ch.cw * L * 4, nrows, cudaMemcpyHostToDevice, s_h2d_),
+                       "H2D");
+        else
+            cuda_check(cudaMemcpyAsync(d_in_[P] + off, h_in_[P] + off, words * 4, cudaMemcpyHostToDevice, s_h2d_),
+                       "H2D");
         cuda_check(cudaEventRecord(ev_in_[i], s_h2d_), "record");
         mark("h2d" + std::to_string(i), s_h2d_);
         cuda_check(cudaStreamWaitEvent(sc, ev_in_[i], 0), "wait");
@@ -843,8 +922,8 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     launch_rows(true, d_rb_, d_ra_, 1, s0);
     cuda_check(cudaEventRecord(ev_fused_, s0), "record");
     mark("fused", s0);
-    for (size_t oc = 0; oc < cout_.size(); ++oc) {
-        const Chunk ch = cout_[oc];
+    for (size_t oc = 0; oc < cout.size(); ++oc) {
+        const Chunk ch = cout[oc];
         const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
         cudaStream_t sc = s_comp_[oc % 3];
         if (oc % 3 != 0) cuda_check(cudaStreamWaitEvent(sc, ev_fused_, 0), "wait");
@@ -854,21 +933,28 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         cuda_check(cudaEventRecord(ev_crt_[oc], sc), "record");
         mark("crt" + std::to_string(oc), sc);
         cuda_check(cudaStreamWaitEvent(s_d2h_, ev_crt_[oc], 0), "wait");
-        cuda_check(cudaMemcpyAsync(h_out_ + off, d_out_ + off, words * 4, cudaMemcpyDeviceToHost, s_d2h_), "D2H");
+        if (direct_out)
+            cuda_check(cudaMemcpy2DAsync(c + (size_t)ch.col0 * L, pitch, d_out_ + off, (size_t)ch.cw * L * 4,
+                                         (size_t)ch.cw * L * 4, nrows, cudaMemcpyDeviceToHost, s_d2h_),
+                       "D2H");
+        else
+            cuda_check(cudaMemcpyAsync(h_out_ + off, d_out_ + off, words * 4, cudaMemcpyDeviceToHost, s_d2h_),
+                       "D2H");
         cuda_check(cudaEventRecord(ev_out_[oc], s_d2h_), "record");
         mark("d2h" + std::to_string(oc), s_d2h_);
     }
     // device status word -> pinned memory behind the last D2H (s_d2h has waited on every CRT)
     cuda_check(cudaMemcpyAsync(h_status_, dp_.status, 4, cudaMemcpyDeviceToHost, s_d2h_), "status D2H");
     cuda_check(cudaMemsetAsync(dp_.status, 0, 4, s_d2h_), "status clear");
-    cuda_check(cudaEventRecord(ev_out_.back(), s_d2h_), "record");
+    cuda_check(cudaEventRecord(ev_out_[cout.size() - 1], s_d2h_), "record");  // re-recorded: the host waits on it
     cuda_check(cudaGetLastError(), "kernel launch");
     t_inputs = clk::now();
-    for (size_t oc = 0; oc < cout_.size(); ++oc) {
+    for (size_t oc = 0; oc < cout.size(); ++oc) {
         cuda_check(cudaEventSynchronize(ev_out_[oc]), "D2H chunk");
         if (oc == 0) t_first_out = clk::now();
-        if (oc + 1 == cout_.size()) t_last_out = clk::now();
-        const Chunk ch = cout_[oc];
+        if (oc + 1 == cout.size()) t_last_out = clk::now();
+        if (direct_out) continue;
+        const Chunk ch = cout[oc];
         const uint32_t* srcc = h_out_ + (size_t)ch.col0 * nrows * L;
         const size_t seg = (size_t)ch.cw * L;
         pool_->run((int)ntasks, [&](int t) {
@@ -879,8 +965,10 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     }
     if (profile_) {
         std::fprintf(stderr,
-                     "polymult: host: stage0 %.1f us | inputs issued %.1f | first out %.1f | last out %.1f | done %.1f\n",
-                     us(t_stage0), us(t_inputs), us(t_first_out), us(t_last_out), us(clk::now()));
+                     "polymult: host: stage0 %.1f us | inputs issued %.1f | first out %.1f | last out %.1f | done %.1f"
+                     " | direct copies a %d b %d c %d\n",
+                     us(t_stage0), us(t_inputs), us(t_first_out), us(t_last_out), us(clk::now()), (int)direct_in[0],
+                     (int)direct_in[1], (int)direct_out);
         std::string line = "polymult: device (us after start):";
         for (size_t k = 1; k < marks.size(); ++k) {
             float ms = 0;

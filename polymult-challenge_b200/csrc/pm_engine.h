@@ -102,11 +102,13 @@ class Engine {
     // called before a CUDA-graph capture so that no allocation happens inside it.
     void reserve(size_t coeffs) { reserve_crt_partials(coeffs); }
     // Host pipeline column-chunk schedule (powers of two: body chunks of ncols / divisor).
-    void set_chunk_schedule(uint32_t in_body, uint32_t out_body);
+    // Host-pipeline schedules per kind of call: kind 0 = operands staged through the host pool
+    // (pageable buffers), kind 1 = operands and result page-locked, moved by direct copies.
+    void set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind = 0);
     // Measures the candidate schedules on run_host and keeps the fastest; median ms.
-    double tune_host_pipeline(int reps);
-    uint32_t in_body() const { return in_body_; }
-    uint32_t out_body() const { return out_body_; }
+    double tune_host_pipeline(int reps, int kind = 0);
+    uint32_t in_body(int kind = 0) const { return in_body_[kind]; }
+    uint32_t out_body(int kind = 0) const { return out_body_[kind]; }
     // Reads (and clears) the device status word; synchronises with the device.
     uint32_t take_status();
     void throw_if_status();
@@ -119,8 +121,8 @@ class Engine {
     size_t table_bytes() const { return table_bytes_; }
     uint32_t group() const { return group_cap_; }  // multiplies per launch group of run_device
     int kernel_launches_per_group() const;
-    const std::vector<Chunk>& in_chunks() const { return cin_; }
-    const std::vector<Chunk>& out_chunks() const { return cout_; }
+    const std::vector<Chunk>& in_chunks(int kind = 0) const { return cin_[kind]; }
+    const std::vector<Chunk>& out_chunks(int kind = 0) const { return cout_[kind]; }
 
     // launch helpers (also used by the tests' stage-by-stage checks)
     void launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s) const;
@@ -183,8 +185,8 @@ class Engine {
     bool dec_tab_smem_ = false;
 
     // host pipeline
-    std::vector<Chunk> cin_, cout_;
-    uint32_t in_body_ = 8, out_body_ = 8;
+    std::vector<Chunk> cin_[2], cout_[2];
+    uint32_t in_body_[2] = {8, 8}, out_body_[2] = {8, 8};
     uint32_t* d_in_[2] = {nullptr, nullptr};
     uint32_t* d_out_ = nullptr;
     uint32_t* h_in_[2] = {nullptr, nullptr};

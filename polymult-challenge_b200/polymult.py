@@ -70,6 +70,7 @@ class PmBatchClassInfo(ctypes.Structure):
 
 
 BATCH_TUNE, BATCH_NO_GRAPH = 1, 2
+PIPELINE_PINNED = 1
 
 
 class PmServeStats(ctypes.Structure):
@@ -119,9 +120,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_plan_selfcheck.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp,
                                       ctypes.POINTER(ctypes.c_int32)]
     lib.pm_plan_selfcheck.restype = ctypes.c_int
-    lib.pm_tune_pipeline.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
+    lib.pm_tune_pipeline.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
     lib.pm_tune_pipeline.restype = ctypes.c_int
-    lib.pm_get_pipeline.argtypes = [vp, ctypes.POINTER(PmPipelineInfo)]
+    lib.pm_get_pipeline.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
     lib.pm_get_pipeline.restype = ctypes.c_int
     lib.pm_batch_init.argtypes = [ctypes.POINTER(PmBatchClass), ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.POINTER(vp)]
@@ -220,15 +221,16 @@ class Multiplier:
     def sync(self):
         _check(load().pm_sync(self._h))
 
-    def tune_pipeline(self, reps: int = 5) -> dict:
-        """Chooses the host pipeline's chunk schedule by measurement (pm_tune_pipeline)."""
+    def tune_pipeline(self, reps: int = 5, pinned: bool = False) -> dict:
+        """Chooses the host pipeline's chunk schedule by measurement (pm_tune_pipeline): for calls
+        on pageable buffers, or with pinned=True for calls whose a, b and c are page-locked."""
         inf = PmPipelineInfo()
-        _check(load().pm_tune_pipeline(self._h, reps, ctypes.byref(inf)))
+        _check(load().pm_tune_pipeline(self._h, reps, PIPELINE_PINNED if pinned else 0, ctypes.byref(inf)))
         return {f: getattr(inf, f) for f, _ in PmPipelineInfo._fields_}
 
-    def pipeline(self) -> dict:
+    def pipeline(self, pinned: bool = False) -> dict:
         inf = PmPipelineInfo()
-        _check(load().pm_get_pipeline(self._h, ctypes.byref(inf)))
+        _check(load().pm_get_pipeline(self._h, PIPELINE_PINNED if pinned else 0, ctypes.byref(inf)))
         return {f: getattr(inf, f) for f, _ in PmPipelineInfo._fields_}
 
     def close(self):

@@ -9,8 +9,9 @@ chunks the inverse column pass and CRT once per chunk; the row passes launch onc
 this script runs `count` multiplies through pm_run_device and checks the device status.
 Select the device-resident launch of a kernel with ncu's -k / -s (skip the warm-up launches):
     ncu --set full --clock-control none -k regex:k_crt_tc -s 20 -c 1 python .../profile_case.py
---host H then runs H multiplies through pm_run (host operands, the chunked PCIe pipeline);
-with POLYMULT_PROFILE=1 in the environment each call prints its host and device timeline.
+--host H then runs H multiplies through pm_run (host operands, the chunked PCIe pipeline;
+--pinned puts them in page-locked memory, which pm_run copies directly); with
+POLYMULT_PROFILE=1 in the environment each call prints its host and device timeline.
 """
 import argparse
 import os
@@ -26,6 +27,7 @@ def main():
     ap.add_argument("--gemm", default="tensor")
     ap.add_argument("--count", type=int, default=1)
     ap.add_argument("--host", type=int, default=0)
+    ap.add_argument("--pinned", action="store_true", help="host operands and result in page-locked memory")
     a = ap.parse_args()
     import numpy as np
     import torch
@@ -43,9 +45,16 @@ def main():
                           torch.cuda.current_stream().cuda_stream)
         m.sync()
         if a.host:
-            a0 = np.ascontiguousarray(ops[0])
-            b0 = np.ascontiguousarray(ops[a.count])
-            out = np.empty((a.N, L), dtype=np.uint32)
+            if a.pinned:
+                def buf():
+                    return torch.empty((a.N, L), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+                a0, b0, out = buf(), buf(), buf()
+                a0[:] = ops[0]
+                b0[:] = ops[a.count]
+            else:
+                a0 = np.ascontiguousarray(ops[0])
+                b0 = np.ascontiguousarray(ops[a.count])
+                out = np.empty((a.N, L), dtype=np.uint32)
             for _ in range(a.host):
                 m.multiply(a0, b0, out)
             if not np.array_equal(out, dc[0].cpu().numpy().view(np.uint32)):

@@ -111,6 +111,7 @@ def test_batch_server_pipeline_argument_checks():
     assert "resident" in lib.pm_last_error().decode()
     assert lib.pm_server_run(None, 0, None, None, None, None, None, None) == polymult.PM_ERR_INVALID
     lib.pm_server_free(None)
-    assert lib.pm_tune_pipeline(None, 3, None) == polymult.PM_ERR_INVALID
-    assert lib.pm_get_pipeline(None, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_tune_pipeline(None, 3, 0, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_tune_pipeline(None, 3, polymult.PIPELINE_PINNED, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_get_pipeline(None, 0, None) == polymult.PM_ERR_INVALID
 

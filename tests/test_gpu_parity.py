@@ -152,9 +152,60 @@ def test_tuned_pipeline_still_bit_exact():
         info = m.tune_pipeline(2)
         assert info["in_body"] in (4, 8, 16) and info["out_body"] in (4, 8, 16) and info["tuned_ms"] > 0
         assert m.pipeline() == info
+        # the page-locked schedule is tuned on its own and leaves the staged one alone
+        assert m.pipeline(pinned=True)["tuned_ms"] == 0
+        pinfo = m.tune_pipeline(2, pinned=True)
+        assert pinfo["in_body"] in (4, 8, 16) and pinfo["out_body"] in (4, 8, 16) and pinfo["tuned_ms"] > 0
+        assert m.pipeline(pinned=True) == pinfo and m.pipeline() == info
         for case in pt["cases"]:
             a, b, _ = regen_case(pt, case)
             assert sha(m.multiply(a, b)) == case["c_sha256"], (case["s"], case["mode"])
+        m.sync()
+
+
+@pytest.mark.parametrize("nw", [(4096, 256), (32768, 868), (65536, 1747)], ids=lambda x: "N%d_W%d" % x)
+def test_pinned_host_operands_take_direct_copies(nw):
+    """Host operands already in page-locked memory skip the host staging: pm_run moves each
+    column chunk with one strided DMA copy in and out.  Every mix of pinned and pageable
+    operands and result gives the reference's bytes (narrow chunks of a few columns included
+    at N = 4096)."""
+    torch = _torch()
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == nw)
+    N, L = pt["N"], pt["L"]
+
+    def pinned(x=None):
+        buf = torch.empty((N, L), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        buf[:] = 0 if x is None else x
+        return buf
+
+    with _multiplier(pt, "tensor") as m:
+        for case in pt["cases"][:2]:
+            a, b, _ = regen_case(pt, case)
+            for pa, pb, pc in [(1, 1, 1), (1, 0, 0), (0, 1, 1), (0, 0, 1)]:
+                ha = pinned(a) if pa else np.ascontiguousarray(a)
+                hb = pinned(b) if pb else np.ascontiguousarray(b)
+                hc = pinned() if pc else np.zeros((N, L), dtype=np.uint32)
+                m.multiply(ha, hb, hc)
+                assert sha(hc) == case["c_sha256"], (case["s"], case["mode"], pa, pb, pc)
+        m.sync()
+
+
+def test_pinned_operands_are_detected(monkeypatch, capfd):
+    """The direct-copy path is taken exactly for the page-locked buffers (POLYMULT_PROFILE's
+    per-call line names which of a, b and c moved by direct copies)."""
+    torch = _torch()
+    monkeypatch.setenv("POLYMULT_PROFILE", "1")
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (32768, 868))
+    N, L = pt["N"], pt["L"]
+    a, b, _ = regen_case(pt, pt["cases"][0])
+    pa = torch.empty((N, L), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    pa[:] = a
+    with _multiplier(pt, "tensor") as m:
+        capfd.readouterr()
+        c = m.multiply(pa, np.ascontiguousarray(b))
+        err = capfd.readouterr().err
+        assert "direct copies a 1 b 0 c 0" in err, err
+        assert sha(c) == pt["cases"][0]["c_sha256"]
         m.sync()
 
 
