@@ -4,11 +4,14 @@
 // Same transform as the reference (psi-merged Cooley-Tukey forward, natural order in and
 // bit-reversed out; Gentleman-Sande inverse with the mirrored-twiddle identity
 // psi^-bitrev(2^s+i) = -psi^bitrev(2^s+2^s-1-i); solve.cu:204-378), organised differently:
-//   * every stage uses Harvey lazy butterflies and Montgomery-Shoup twiddle products
-//     (pm_device.cuh), so no butterfly reduces to [0, p);
-//   * twiddles come from one table tw[j][k] = psi_j^bitrev(k) R (mod p_j), read directly
-//     (row pass) or staged once per CTA with their Shoup companions (column pass), instead of
-//     forming trow * tsmall with a Montgomery product at every butterfly (solve.cu:286-338);
+//   * every stage uses Harvey lazy butterflies (pm_device.cuh), so no butterfly reduces to
+//     [0, p): Montgomery-Shoup twiddle products in the row pass, Shoup products (one integer
+//     instruction fewer) in the column pass;
+//   * twiddles come from one table tw[j][k] = psi_j^bitrev(k) R (mod p_j), read directly in
+//     vector runs (row pass: a stage's 2^t twiddles of a thread are consecutive), and from its
+//     first nrows entries in Shoup form {psi^bitrev(k), floor(psi^bitrev(k) 2^32 / p)} staged
+//     once per CTA (column pass), instead of forming trow * tsmall with a Montgomery product
+//     at every butterfly (solve.cu:286-338);
 //   * a line of 2^NB elements is transformed in PHASES of up to RB = 4 stages.  In a phase a
 //     thread holds 16 elements of the line in registers -- the 16 values of the 4 index bits
 //     [b0, b0 + 4) that the phase's stages pair up -- and runs a radix-16 butterfly network on
@@ -39,36 +42,83 @@ struct LineCfg {
     __host__ __device__ static constexpr int ls(int k, int t) { return NB - b0(k) - RB + t; }
 };
 
-// Forward (CT) radix network on v[] over local stages t0..RB-1 of one phase; tw(t, gi)
-// returns the twiddle of local stage t, group gi = (hi << t) | m (hi is folded in by tw).
-template <int RB, int T0, class TwF>
-__device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const TwF& tw, uint32_t p) {
+// Forward (CT) radix network on v[] over local stages t0..RB-1 of one phase.  stw(t) returns
+// the stage's twiddle source: w[m] is the Tw2 of group m (gi = (hi << t) | m; hi is folded in
+// by stw).  SH: the twiddles are in Shoup form {w, floor(w 2^32 / p)}, else Montgomery-Shoup
+// {wR, wR p^-1}.
+template <int RB, int T0, bool SH, class StwF>
+__device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const StwF& stw, uint32_t p) {
 #pragma unroll
     for (int t = T0; t < RB; ++t) {
         const int h = (1 << RB) >> (t + 1);
+        const auto w = stw(t);
 #pragma unroll
         for (int m = 0; m < (1 << t); ++m) {
-            const Tw2 w = tw(t, m);
+            const Tw2 wm = w[m];
 #pragma unroll
-            for (int i = 0; i < h; ++i) bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
+            for (int i = 0; i < h; ++i) {
+                if (SH) bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                else bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+            }
         }
     }
 }
 
-// Inverse (GS) network, local stages RB-1 down to T0, mirrored twiddles from tw(t, m).
-template <int RB, int T0, class TwF>
-__device__ __forceinline__ void radix_inv(uint32_t (&v)[1 << RB], const TwF& tw, uint32_t p) {
+// Inverse (GS) network, local stages RB-1 down to T0, mirrored twiddles from stw(t).
+template <int RB, int T0, bool SH, class StwF>
+__device__ __forceinline__ void radix_inv(uint32_t (&v)[1 << RB], const StwF& stw, uint32_t p) {
 #pragma unroll
     for (int t = RB - 1; t >= T0; --t) {
         const int h = (1 << RB) >> (t + 1);
+        const auto w = stw(t);
 #pragma unroll
         for (int m = 0; m < (1 << t); ++m) {
-            const Tw2 w = tw(t, m);
+            const Tw2 wm = w[m];
 #pragma unroll
-            for (int i = 0; i < h; ++i) bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], w, p);
+            for (int i = 0; i < h; ++i) {
+                if (SH) bfly_gs_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                else bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+            }
         }
     }
 }
+
+// A stage's run of 2^t (t < 4) consecutive table words starting at `src`, aligned to 2^t
+// words, read with as few vector loads as the run allows.  w[m] is word m (REV: word
+// 2^t - 1 - m) with its Montgomery-Shoup companion formed at use.
+template <bool REV>
+struct RunTw {
+    uint32_t x[8];
+    uint32_t pinv;
+    int n;
+    __device__ __forceinline__ RunTw(const uint32_t* src, int t, uint32_t pi) : pinv(pi), n(1 << t) {
+        if (t == 0) {
+            x[0] = __ldg(src);
+        } else if (t == 1) {
+            const uint2 u = __ldg(reinterpret_cast<const uint2*>(src));
+            x[0] = u.x;
+            x[1] = u.y;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (q == 1 && t < 3) break;
+                const uint4 u = __ldg(reinterpret_cast<const uint4*>(src) + q);
+                x[4 * q] = u.x;
+                x[4 * q + 1] = u.y;
+                x[4 * q + 2] = u.z;
+                x[4 * q + 3] = u.w;
+            }
+        }
+    }
+    __device__ __forceinline__ Tw2 operator[](int m) const { return make_tw(x[REV ? n - 1 - m : m], pinv); }
+};
+
+// A column stage's twiddles in shared memory (Shoup form): w[m] = base[m] or, REV, base[-m].
+template <bool REV>
+struct SmemTw {
+    const Tw2* base;
+    __device__ __forceinline__ Tw2 operator[](int m) const { return base[REV ? -m : m]; }
+};
 
 // ---------------------------------------------------------------------------------------
 // Row pass layout.  LPR = 2^(NB-RB) threads share a row; a shared-memory region serves
@@ -188,12 +238,13 @@ __device__ __forceinline__ void row_forward(uint32_t (&v)[RowCfg<NB>::E], uint32
     if constexpr (K < C::NPH) {
         constexpr int b0 = C::b0(K);
         const uint32_t hip = (uint32_t)(r >> b0);  // index bits above the registers
-        // per local stage t: the row's run of twiddles, tw[2^(w1+ls) + hi 2^ls + (hip << t) + m]
-        auto tw = [&](int t, int m) {
+        // per local stage t: the row's run of twiddles, tw[2^(w1+ls) + hi 2^ls + (hip << t) + m],
+        // m < 2^t: 2^t consecutive words aligned to 2^t (ls >= t)
+        auto stw = [&](int t) {
             const int ls = C::ls(K, t);
-            return make_tw(__ldg(twj + (1u << (w1 + ls)) + (hi << ls) + ((hip << t) | (uint32_t)m)), pinv);
+            return RunTw<false>(twj + (1u << (w1 + ls)) + (hi << ls) + (hip << t), t, pinv);
         };
-        radix_fwd<C::RB, C::t0(K)>(v, tw, p);
+        radix_fwd<C::RB, C::t0(K), false>(v, stw, p);
         if constexpr (K + 1 < C::NPH) {
             row_xchg<NB, K, true>(v, region, rho, r);
             region_sync<NB>();
@@ -214,13 +265,13 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
     if constexpr (K >= 0) {
         constexpr int b0 = C::b0(K);
         const uint32_t hip = (uint32_t)(r >> b0);
-        // tw[2^(w1+ls) + hi_m 2^ls + 2^ls - 1 - ((hip << t) + m)]
-        auto tw = [&](int t, int m) {
+        // tw[2^(w1+ls) + hi_m 2^ls + 2^ls - 1 - ((hip << t) + m)], m < 2^t: the aligned run of 2^t
+        // words ending there, read in reverse
+        auto stw = [&](int t) {
             const int ls = C::ls(K, t);
-            const uint32_t gi = (hip << t) | (uint32_t)m;
-            return make_tw(__ldg(twj + (1u << (w1 + ls)) + (hi_m << ls) + ((1u << ls) - 1u - gi)), pinv);
+            return RunTw<true>(twj + (1u << (w1 + ls)) + (hi_m << ls) + (1u << ls) - ((hip + 1u) << t), t, pinv);
         };
-        radix_inv<C::RB, C::t0(K)>(v, tw, p);
+        radix_inv<C::RB, C::t0(K), false>(v, stw, p);
         if constexpr (K > 0) {
             row_xchg<NB, K, true>(v, region, rho, r);
             region_sync<NB>();
@@ -242,7 +293,7 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
 //                  transform ra_sel[z] of RA when ra_sel is given (a server's resident
 //                  operands), else with transform z.
 template <int NB, bool FUSED>
-__global__ void __launch_bounds__(128, 8) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
+__global__ void __launch_bounds__(128, NB >= 9 ? 5 : 8) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
                                                   const uint32_t* __restrict__ ra_sel) {
     using C = RowCfg<NB>;
     __shared__ __align__(16) uint32_t sh[C::NPH > 1 ? 128 * C::E : 4];
@@ -283,8 +334,8 @@ __global__ void __launch_bounds__(128, 8) k_ntt_rows(DevPlan P, uint32_t* __rest
 // register bits.  Phase 0 (forward) reads its groups straight from global memory and the last
 // phase writes straight back; the tile in shared memory ([row][TC], a warp touching 32
 // consecutive columns of one row) carries the values between phases.  Column stage s, group
-// i uses tw[2^s + i] (forward) or tw[2^(s+1) - 1 - i] (inverse), staged once per CTA with its
-// Shoup companion.
+// i uses tw[2^s + i] (forward) or tw[2^(s+1) - 1 - i] (inverse), staged once per CTA in Shoup
+// form from the plan's twsh table.
 // ---------------------------------------------------------------------------------------
 namespace {
 
@@ -315,11 +366,11 @@ __device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32
         for (int t = 0; t < C::RB; ++t)
             tb[t] = INV ? (2 << C::ls(K, t)) - 1 - (hip << t) : (1 << C::ls(K, t)) + (hip << t);
         if (!INV) {
-            auto tw = [&](int t, int m) { return tws[tb[t] + m]; };
-            radix_fwd<C::RB, C::t0(K)>(v, tw, p);
+            auto stw = [&](int t) { return SmemTw<false>{tws + tb[t]}; };
+            radix_fwd<C::RB, C::t0(K), true>(v, stw, p);
         } else {
-            auto tw = [&](int t, int m) { return tws[tb[t] - m]; };
-            radix_inv<C::RB, C::t0(K)>(v, tw, p);
+            auto stw = [&](int t) { return SmemTw<true>{tws + tb[t]}; };
+            radix_inv<C::RB, C::t0(K), true>(v, stw, p);
         }
 #pragma unroll
         for (int e = 0; e < C::E; ++e) {
@@ -352,10 +403,13 @@ __global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restric
     Tw2* tws = reinterpret_cast<Tw2*>(smem_raw);            // [NR]
     uint32_t* tile = reinterpret_cast<uint32_t*>(tws + NR);  // [NR][TC]
     const int j = (int)blockIdx.y;
-    const uint32_t p = P.p[j], pinv = P.pinv[j];
+    const uint32_t p = P.p[j];
     uint32_t* base = R + ((size_t)blockIdx.z * P.K + j) * P.N + col0 + ((uint32_t)blockIdx.x << ltc);
-    const uint32_t* tw = P.tw + (size_t)j * P.N;
-    for (int k = threadIdx.x; k < NR; k += blockDim.x) tws[k] = make_tw(__ldg(tw + k), pinv);
+    const uint2* tw = P.twsh + (size_t)j * NR;
+    for (int k = threadIdx.x; k < NR; k += blockDim.x) {
+        const uint2 u = __ldg(tw + k);
+        tws[k] = Tw2{u.x, u.y};
+    }
     __syncthreads();
     col_phases<NB, INV, 0>(tile, tws, base, P.ncols, ltc, p);
 }

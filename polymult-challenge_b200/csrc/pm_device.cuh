@@ -34,6 +34,7 @@ struct DevPlan {
     const uint32_t* crt_cc;   // [KP]
     const float* rcp;         // [KP]
     const uint32_t* tw;       // [K][N] Montgomery-form psi^bitrev(k)
+    const uint2* twsh;        // [K][nrows] {psi^bitrev(k), floor(psi^bitrev(k) 2^32 / p)}, k < nrows
     const uint32_t* dec16;    // [2L][KP]
     const uint16_t* qh16;     // [KP][HP]
     const uint32_t* tneg;     // [K+1][L]
@@ -91,6 +92,30 @@ __device__ __forceinline__ void bfly_ct(uint32_t& x, uint32_t& y, Tw2 w, uint32_
     const uint32_t t = mul_ms(y, w.w, w.wc, p);
     x = xr + t;
     y = xr - t + p2;
+}
+
+// Shoup product: x * w mod p in [0, 2p) for any x < 2^32, w < p plain and wsh = floor(w 2^32 / p)
+// (the quotient estimate umulhi(x, wsh) is at most one below floor(x w / p)).
+__device__ __forceinline__ uint32_t mul_sh(uint32_t x, uint32_t w, uint32_t wsh, uint32_t p) {
+    return x * w - __umulhi(x, wsh) * p;
+}
+
+// Cooley-Tukey butterfly with a Shoup twiddle {w, wsh}: x, y in [0, 4p) -> [0, 4p).
+__device__ __forceinline__ void bfly_ct_sh(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
+    const uint32_t p2 = 2 * p;
+    const uint32_t xr = red_once(x, p2);
+    const uint32_t t = mul_sh(y, w.w, w.wc, p);
+    x = xr + t;
+    y = xr - t + p2;
+}
+
+// Gentleman-Sande butterfly with a Shoup twiddle: x, y in [0, 2p) -> [0, 2p).
+__device__ __forceinline__ void bfly_gs_sh(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
+    const uint32_t p2 = 2 * p;
+    const uint32_t s = x + y;
+    const uint32_t d = y - x + p2;
+    x = red_once(s, p2);
+    y = mul_sh(d, w.w, w.wc, p);
 }
 
 // Gentleman-Sande (inverse) butterfly with the mirrored twiddle: x, y in [0, 2p) ->
