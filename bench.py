@@ -569,8 +569,9 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu, cref = reference_cpu(N, W, q, a0, b0, calls=1, warm=0)
-        cpu["matches_gpu"] = bool(np.array_equal(cref, out))
+        cpu, cref = reference_cpu(N, W, q, np.ascontiguousarray(host_a[0]), np.ascontiguousarray(host_b[0]),
+                                  calls=1, warm=0)
+        cpu["matches_gpu"] = bool(np.array_equal(cref, want))
 
     m.close()
     mp.close()

@@ -4,14 +4,12 @@
 // Same transform as the reference (psi-merged Cooley-Tukey forward, natural order in and
 // bit-reversed out; Gentleman-Sande inverse with the mirrored-twiddle identity
 // psi^-bitrev(2^s+i) = -psi^bitrev(2^s+2^s-1-i); solve.cu:204-378), organised differently:
-//   * every stage uses Harvey lazy butterflies (pm_device.cuh), so no butterfly reduces to
-//     [0, p): Montgomery-Shoup twiddle products in the row pass, Shoup products (one integer
-//     instruction fewer) in the column pass;
-//   * twiddles come from one table tw[j][k] = psi_j^bitrev(k) R (mod p_j), read directly in
-//     vector runs (row pass: a stage's 2^t twiddles of a thread are consecutive), and from its
-//     first nrows entries in Shoup form {psi^bitrev(k), floor(psi^bitrev(k) 2^32 / p)} staged
-//     once per CTA (column pass), instead of forming trow * tsmall with a Montgomery product
-//     at every butterfly (solve.cu:286-338);
+//   * every stage uses Harvey lazy butterflies with Shoup twiddle products (pm_device.cuh), so
+//     no butterfly reduces to [0, p);
+//   * twiddles come from one table tw[j][k] = {psi_j^bitrev(k), floor(psi_j^bitrev(k) 2^32 / p_j)},
+//     read directly in 16-byte runs (row pass: a stage's 2^t twiddles of a thread are
+//     consecutive) or staged once per CTA (column pass: the first nrows entries), instead of
+//     forming trow * tsmall with a Montgomery product at every butterfly (solve.cu:286-338);
 //   * a line of 2^NB elements is transformed in PHASES of up to RB = 4 stages.  In a phase a
 //     thread holds 16 elements of the line in registers -- the 16 values of the 4 index bits
 //     [b0, b0 + 4) that the phase's stages pair up -- and runs a radix-16 butterfly network on
@@ -43,10 +41,9 @@ struct LineCfg {
 };
 
 // Forward (CT) radix network on v[] over local stages t0..RB-1 of one phase.  stw(t) returns
-// the stage's twiddle source: w[m] is the Tw2 of group m (gi = (hi << t) | m; hi is folded in
-// by stw).  SH: the twiddles are in Shoup form {w, floor(w 2^32 / p)}, else Montgomery-Shoup
-// {wR, wR p^-1}.
-template <int RB, int T0, bool SH, class StwF>
+// the stage's twiddle source: w[m] is the Shoup-form Tw2 {w, floor(w 2^32 / p)} of group m
+// (gi = (hi << t) | m; hi is folded in by stw).
+template <int RB, int T0, class StwF>
 __device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const StwF& stw, uint32_t p) {
 #pragma unroll
     for (int t = T0; t < RB; ++t) {
@@ -57,15 +54,14 @@ __device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const StwF& st
             const Tw2 wm = w[m];
 #pragma unroll
             for (int i = 0; i < h; ++i) {
-                if (SH) bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
-                else bfly_ct(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
             }
         }
     }
 }
 
 // Inverse (GS) network, local stages RB-1 down to T0, mirrored twiddles from stw(t).
-template <int RB, int T0, bool SH, class StwF>
+template <int RB, int T0, class StwF>
 __device__ __forceinline__ void radix_inv(uint32_t (&v)[1 << RB], const StwF& stw, uint32_t p) {
 #pragma unroll
     for (int t = RB - 1; t >= T0; --t) {
@@ -76,41 +72,29 @@ __device__ __forceinline__ void radix_inv(uint32_t (&v)[1 << RB], const StwF& st
             const Tw2 wm = w[m];
 #pragma unroll
             for (int i = 0; i < h; ++i) {
-                if (SH) bfly_gs_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
-                else bfly_gs(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                bfly_gs_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
             }
         }
     }
 }
 
-// A stage's run of 2^t (t < 4) consecutive table words starting at `src`, aligned to 2^t
-// words, read with as few vector loads as the run allows.  w[m] is word m (REV: word
-// 2^t - 1 - m) with its Montgomery-Shoup companion formed at use.
+// A stage's run of 2^t consecutive Shoup-form twiddles {w, floor(w 2^32 / p)} starting at
+// `src`, aligned to 2^t entries.  w[m] is entry m (REV: entry 2^t - 1 - m), read at use as
+// half of a 16-byte pair (the two entries of a pair come from one load), so that no more of
+// the run than the current butterflies need is held in registers.
 template <bool REV>
 struct RunTw {
-    uint32_t x[8];
-    uint32_t pinv;
+    const uint2* src;
     int n;
-    __device__ __forceinline__ RunTw(const uint32_t* src, int t, uint32_t pi) : pinv(pi), n(1 << t) {
-        if (t == 0) {
-            x[0] = __ldg(src);
-        } else if (t == 1) {
-            const uint2 u = __ldg(reinterpret_cast<const uint2*>(src));
-            x[0] = u.x;
-            x[1] = u.y;
-        } else {
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                if (q == 1 && t < 3) break;
-                const uint4 u = __ldg(reinterpret_cast<const uint4*>(src) + q);
-                x[4 * q] = u.x;
-                x[4 * q + 1] = u.y;
-                x[4 * q + 2] = u.z;
-                x[4 * q + 3] = u.w;
-            }
+    __device__ __forceinline__ Tw2 operator[](int m) const {
+        const int e = REV ? n - 1 - m : m;
+        if (n == 1) {
+            const uint2 u = __ldg(src);
+            return Tw2{u.x, u.y};
         }
+        const uint4 u = __ldg(reinterpret_cast<const uint4*>(src) + (e >> 1));
+        return (e & 1) ? Tw2{u.z, u.w} : Tw2{u.x, u.y};
     }
-    __device__ __forceinline__ Tw2 operator[](int m) const { return make_tw(x[REV ? n - 1 - m : m], pinv); }
 };
 
 // A column stage's twiddles in shared memory (Shoup form): w[m] = base[m] or, REV, base[-m].
@@ -233,7 +217,7 @@ __device__ __forceinline__ void row_global(uint32_t (&v)[RowCfg<NB>::E], uint32_
 // NPH-1 on exit).  Stage ls of row hi, group gi uses tw[2^(w1+ls) + hi 2^ls + gi].
 template <int NB, int K>
 __device__ __forceinline__ void row_forward(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r,
-                                            const uint32_t* twj, int w1, uint32_t hi, uint32_t p, uint32_t pinv) {
+                                            const uint2* twj, int w1, uint32_t hi, uint32_t p) {
     using C = RowCfg<NB>;
     if constexpr (K < C::NPH) {
         constexpr int b0 = C::b0(K);
@@ -242,15 +226,15 @@ __device__ __forceinline__ void row_forward(uint32_t (&v)[RowCfg<NB>::E], uint32
         // m < 2^t: 2^t consecutive words aligned to 2^t (ls >= t)
         auto stw = [&](int t) {
             const int ls = C::ls(K, t);
-            return RunTw<false>(twj + (1u << (w1 + ls)) + (hi << ls) + (hip << t), t, pinv);
+            return RunTw<false>{twj + (1u << (w1 + ls)) + (hi << ls) + (hip << t), 1 << t};
         };
-        radix_fwd<C::RB, C::t0(K), false>(v, stw, p);
+        radix_fwd<C::RB, C::t0(K)>(v, stw, p);
         if constexpr (K + 1 < C::NPH) {
             row_xchg<NB, K, true>(v, region, rho, r);
             region_sync<NB>();
             row_xchg<NB, K + 1, false>(v, region, rho, r);
             region_sync<NB>();
-            row_forward<NB, K + 1>(v, region, rho, r, twj, w1, hi, p, pinv);
+            row_forward<NB, K + 1>(v, region, rho, r, twj, w1, hi, p);
         }
     }
 }
@@ -260,7 +244,7 @@ __device__ __forceinline__ void row_forward(uint32_t (&v)[RowCfg<NB>::E], uint32
 // 2^ls - 1 - gi.
 template <int NB, int K>
 __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r,
-                                            const uint32_t* twj, int w1, uint32_t hi_m, uint32_t p, uint32_t pinv) {
+                                            const uint2* twj, int w1, uint32_t hi_m, uint32_t p) {
     using C = RowCfg<NB>;
     if constexpr (K >= 0) {
         constexpr int b0 = C::b0(K);
@@ -269,31 +253,32 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
         // words ending there, read in reverse
         auto stw = [&](int t) {
             const int ls = C::ls(K, t);
-            return RunTw<true>(twj + (1u << (w1 + ls)) + (hi_m << ls) + (1u << ls) - ((hip + 1u) << t), t, pinv);
+            return RunTw<true>{twj + (1u << (w1 + ls)) + (hi_m << ls) + (1u << ls) - ((hip + 1u) << t), 1 << t};
         };
-        radix_inv<C::RB, C::t0(K), false>(v, stw, p);
+        radix_inv<C::RB, C::t0(K)>(v, stw, p);
         if constexpr (K > 0) {
             row_xchg<NB, K, true>(v, region, rho, r);
             region_sync<NB>();
             row_xchg<NB, K - 1, false>(v, region, rho, r);
             region_sync<NB>();
-            row_inverse<NB, K - 1>(v, region, rho, r, twj, w1, hi_m, p, pinv);
+            row_inverse<NB, K - 1>(v, region, rho, r, twj, w1, hi_m, p);
         }
     }
 }
 
 }  // namespace
 
-// Row pass over ROWS_PER_CTA consecutive rows of prime blockIdx.y, batch blockIdx.z,
-// 128 threads.
+// Row pass over ROWS_PER_CTA consecutive rows of one prime and batch entry, 128 threads.
 //   FUSED = false: forward row stages (operand a).
 //   FUSED = true : forward row stages of b, pointwise product with the finished transform of
 //                  a (RA), inverse row stages.  The Montgomery pointwise product leaves a
 //                  factor 2^-32 that the CRT constant crt_c compensates.  Batch z pairs with
 //                  transform ra_sel[z] of RA when ra_sel is given (a server's resident
 //                  operands), else with transform z.
+// Blocks per SM: the most at which no variant spills (64 registers at 8, 80 at 6, 96 at 5,
+// 128 at 4); the fused kernel holds the other operand's row and more twiddle runs.
 template <int NB, bool FUSED>
-__global__ void __launch_bounds__(128, NB >= 9 ? 5 : 8) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
+__global__ void __launch_bounds__(128, NB >= 9 ? (FUSED ? 4 : 5) : (FUSED ? 6 : 8)) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
                                                   const uint32_t* __restrict__ ra_sel) {
     using C = RowCfg<NB>;
     __shared__ __align__(16) uint32_t sh[C::NPH > 1 ? 128 * C::E : 4];
@@ -301,26 +286,32 @@ __global__ void __launch_bounds__(128, NB >= 9 ? 5 : 8) k_ntt_rows(DevPlan P, ui
     const int li = tid % C::GRP;                 // thread within the shared-memory region
     const int rho = li / C::LPR, r = li % C::LPR;
     uint32_t* region = sh + (tid / C::GRP) * (C::GRP * C::E);
-    const uint32_t hi = blockIdx.x * C::ROWS_PER_CTA + (uint32_t)(tid / C::LPR);
+    // the grid is (row blocks, primes, batch); blocks take them batch entry fastest in launch
+    // order, so the nb blocks of one (row block, prime), which read the same twiddles, run
+    // side by side and share them in L2
+    const uint32_t lin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const uint32_t zb = lin % gridDim.z, rest = lin / gridDim.z;
+    const uint32_t xb = rest % gridDim.x;
+    const int j = (int)(rest / gridDim.x);
+    const uint32_t hi = xb * C::ROWS_PER_CTA + (uint32_t)(tid / C::LPR);
     const bool active = hi < P.nrows;
     const uint32_t hic = active ? hi : P.nrows - 1;  // keeps twiddle reads in range
-    const int j = (int)blockIdx.y;
     const uint32_t p = P.p[j], pinv = P.pinv[j];
-    const size_t off = ((size_t)blockIdx.z * P.K + j) * P.N + (size_t)hic * (1u << NB);
+    const size_t off = ((size_t)zb * P.K + j) * P.N + (size_t)hic * (1u << NB);
     uint32_t* row = R + off;
-    const uint32_t* twj = P.tw + (size_t)j * P.N;
+    const uint2* twj = P.tw + (size_t)j * P.N;
 
     uint32_t v[C::E];
     row_global<NB, 0, true>(v, row, r, active);
-    row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p, pinv);
+    row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p);
     if constexpr (FUSED) {
         uint32_t a[C::E];
-        const size_t za = ra_sel ? (size_t)__ldg(ra_sel + blockIdx.z) : (size_t)blockIdx.z;
+        const size_t za = ra_sel ? (size_t)__ldg(ra_sel + zb) : (size_t)zb;
         const size_t offa = (za * P.K + j) * P.N + (size_t)hic * (1u << NB);
         row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), true>(a, const_cast<uint32_t*>(RA + offa), r, active);
 #pragma unroll
         for (int e = 0; e < C::E; ++e) v[e] = mont_mul(red_once(red_once(a[e], 2 * p), p), v[e], p, pinv);
-        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p, pinv);
+        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p);
         row_global<NB, 0, false>(v, row, r, active);
     } else {
         row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), false>(v, row, r, active);
@@ -334,8 +325,7 @@ __global__ void __launch_bounds__(128, NB >= 9 ? 5 : 8) k_ntt_rows(DevPlan P, ui
 // register bits.  Phase 0 (forward) reads its groups straight from global memory and the last
 // phase writes straight back; the tile in shared memory ([row][TC], a warp touching 32
 // consecutive columns of one row) carries the values between phases.  Column stage s, group
-// i uses tw[2^s + i] (forward) or tw[2^(s+1) - 1 - i] (inverse), staged once per CTA in Shoup
-// form from the plan's twsh table.
+// i uses tw[2^s + i] (forward) or tw[2^(s+1) - 1 - i] (inverse), staged once per CTA.
 // ---------------------------------------------------------------------------------------
 namespace {
 
@@ -367,10 +357,10 @@ __device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32
             tb[t] = INV ? (2 << C::ls(K, t)) - 1 - (hip << t) : (1 << C::ls(K, t)) + (hip << t);
         if (!INV) {
             auto stw = [&](int t) { return SmemTw<false>{tws + tb[t]}; };
-            radix_fwd<C::RB, C::t0(K), true>(v, stw, p);
+            radix_fwd<C::RB, C::t0(K)>(v, stw, p);
         } else {
             auto stw = [&](int t) { return SmemTw<true>{tws + tb[t]}; };
-            radix_inv<C::RB, C::t0(K), true>(v, stw, p);
+            radix_inv<C::RB, C::t0(K)>(v, stw, p);
         }
 #pragma unroll
         for (int e = 0; e < C::E; ++e) {
@@ -405,7 +395,7 @@ __global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restric
     const int j = (int)blockIdx.y;
     const uint32_t p = P.p[j];
     uint32_t* base = R + ((size_t)blockIdx.z * P.K + j) * P.N + col0 + ((uint32_t)blockIdx.x << ltc);
-    const uint2* tw = P.twsh + (size_t)j * NR;
+    const uint2* tw = P.tw + (size_t)j * P.N;
     for (int k = threadIdx.x; k < NR; k += blockDim.x) {
         const uint2 u = __ldg(tw + k);
         tws[k] = Tw2{u.x, u.y};

@@ -33,8 +33,7 @@ struct DevPlan {
     const uint32_t* crt_c;    // [KP]
     const uint32_t* crt_cc;   // [KP]
     const float* rcp;         // [KP]
-    const uint32_t* tw;       // [K][N] Montgomery-form psi^bitrev(k)
-    const uint2* twsh;        // [K][nrows] {psi^bitrev(k), floor(psi^bitrev(k) 2^32 / p)}, k < nrows
+    const uint2* tw;          // [K][N] {psi^bitrev(k), floor(psi^bitrev(k) 2^32 / p)} (Shoup form)
     const uint32_t* dec16;    // [2L][KP]
     const uint16_t* qh16;     // [KP][HP]
     const uint32_t* tneg;     // [K+1][L]
@@ -79,20 +78,10 @@ __device__ __forceinline__ uint32_t redc64(uint64_t t, uint32_t p, uint32_t pinv
 // [0, 2m) -> [0, m) (also [0, 4p) -> [0, 2p) with m = 2p): unsigned min of x and x - m.
 __device__ __forceinline__ uint32_t red_once(uint32_t x, uint32_t m) { return min(x, x - m); }
 
+// A twiddle in Shoup form: w < p and wc = floor(w 2^32 / p).
 struct Tw2 {
     uint32_t w, wc;
 };
-
-__device__ __forceinline__ Tw2 make_tw(uint32_t w, uint32_t pinv) { return Tw2{w, w * pinv}; }
-
-// Cooley-Tukey (forward) Harvey butterfly: x, y in [0, 4p) -> x + wy, x - wy in [0, 4p).
-__device__ __forceinline__ void bfly_ct(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
-    const uint32_t p2 = 2 * p;
-    const uint32_t xr = red_once(x, p2);
-    const uint32_t t = mul_ms(y, w.w, w.wc, p);
-    x = xr + t;
-    y = xr - t + p2;
-}
 
 // Shoup product: x * w mod p in [0, 2p) for any x < 2^32, w < p plain and wsh = floor(w 2^32 / p)
 // (the quotient estimate umulhi(x, wsh) is at most one below floor(x w / p)).
@@ -109,23 +98,14 @@ __device__ __forceinline__ void bfly_ct_sh(uint32_t& x, uint32_t& y, Tw2 w, uint
     y = xr - t + p2;
 }
 
-// Gentleman-Sande butterfly with a Shoup twiddle: x, y in [0, 2p) -> [0, 2p).
+// Gentleman-Sande (inverse) butterfly with the mirrored Shoup twiddle: x, y in [0, 2p) ->
+// x + y, (y - x) w in [0, 2p).  (x - y) psi^-b = (y - x) psi^b' with b + b' = N.
 __device__ __forceinline__ void bfly_gs_sh(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
     const uint32_t p2 = 2 * p;
     const uint32_t s = x + y;
     const uint32_t d = y - x + p2;
     x = red_once(s, p2);
     y = mul_sh(d, w.w, w.wc, p);
-}
-
-// Gentleman-Sande (inverse) butterfly with the mirrored twiddle: x, y in [0, 2p) ->
-// x + y, (y - x) w in [0, 2p).  (x - y) psi^-b = (y - x) psi^b' with b + b' = N.
-__device__ __forceinline__ void bfly_gs(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
-    const uint32_t p2 = 2 * p;
-    const uint32_t s = x + y;
-    const uint32_t d = y - x + p2;
-    x = red_once(s, p2);
-    y = mul_ms(d, w.w, w.wc, p);
 }
 
 __device__ __forceinline__ void flag_error(uint32_t* status, uint32_t bit) {

@@ -335,23 +335,7 @@ void Engine::upload_tables() {
     d.crt_c = dev_upload(dev_allocs_, P.crt_c, tb);
     d.crt_cc = dev_upload(dev_allocs_, P.crt_cc, tb);
     d.rcp = dev_upload(dev_allocs_, P.rcp, tb);
-    d.tw = dev_upload(dev_allocs_, P.tw, tb);
-    {
-        // column-pass twiddles (indices below nrows) in Shoup form: the plain value
-        // psi^bitrev(k) = tw * 2^-32 mod p and floor(value 2^32 / p)
-        std::vector<uint2> sh((size_t)P.K * P.nrows);
-        for (int j = 0; j < P.K; ++j) {
-            const uint64_t p = P.p[j];
-            uint64_t rinv = 1, base = (1ull << 32) % p;  // (2^32)^(p-2) mod p
-            for (uint64_t e = p - 2; e; e >>= 1, base = base * base % p)
-                if (e & 1) rinv = rinv * base % p;
-            for (uint32_t k = 0; k < P.nrows; ++k) {
-                const uint64_t w = (uint64_t)P.tw[(size_t)j * P.N + k] * rinv % p;
-                sh[(size_t)j * P.nrows + k] = make_uint2((uint32_t)w, (uint32_t)((w << 32) / p));
-            }
-        }
-        d.twsh = dev_upload(dev_allocs_, sh, tb);
-    }
+    d.tw = reinterpret_cast<const uint2*>(dev_upload(dev_allocs_, P.tw, tb));
     d.dec16 = dev_upload(dev_allocs_, P.dec16, tb);
     d.qh16 = dev_upload(dev_allocs_, P.qh16, tb);
     d.tneg = dev_upload(dev_allocs_, P.tneg, tb);

@@ -232,7 +232,7 @@ Plan make_plan(uint32_t N, uint32_t W, uint32_t L, const uint32_t* qlimbs) {
     P.crt_c.assign(KP, 0);
     P.crt_cc.assign(KP, 0);
     P.rcp.assign(KP, 0.f);
-    P.tw.assign((size_t)K * N, 0);
+    P.tw.assign((size_t)K * N * 2, 0);
     std::vector<u32> pw(N);
     for (int j = 0; j < KP; ++j) {
         const u32 p = j < K ? primes[j] : primes.back();
@@ -252,8 +252,12 @@ Plan make_plan(uint32_t N, uint32_t W, uint32_t L, const uint32_t* qlimbs) {
         }
         pw[0] = 1;
         for (u32 e = 1; e < N; ++e) pw[e] = (u32)((u64)pw[e - 1] * psi % p);
-        u32* tw = P.tw.data() + (size_t)j * N;
-        for (u32 k = 0; k < N; ++k) tw[k] = (u32)(((u64)pw[bitrev(k, P.logN)] << 32) % p);
+        u32* tw = P.tw.data() + (size_t)j * N * 2;
+        for (u32 k = 0; k < N; ++k) {
+            const u64 w = pw[bitrev(k, P.logN)];
+            tw[2 * k] = (u32)w;
+            tw[2 * k + 1] = (u32)((w << 32) / p);
+        }
         u64 mp = 1;  // (M / p_j) mod p_j
         for (int i = 0; i < K; ++i)
             if (i != j) mp = mp * (primes[i] % p) % p;
@@ -326,14 +330,14 @@ std::string check_plan(const Plan& P) {
         const u32 p = P.p[j];
         if (!is_prime32(p) || p >= (1u << 30) || (p - 1) % P.prime_step != 0) return "bad prime";
         if ((u32)(p * P.pinv[j]) != 1u) return "bad p^-1 mod 2^32";
-        const u64 R = (1ull << 32) % p;
-        const u32* tw = P.tw.data() + (size_t)j * P.N;
-        if (tw[0] != R) return "tw[0] is not 1 in Montgomery form";
-        if (P.N >= 2) {  // tw[1] = psi^(N/2) in Montgomery form: its square is -1
-            const u64 rinv = powmod(R, p - 2, p);
-            const u64 w = (u64)tw[1] * rinv % p;
+        const u32* tw = P.tw.data() + (size_t)j * P.N * 2;
+        if (tw[0] != 1) return "tw[0] is not 1";
+        if (P.N >= 2) {  // tw[1] = psi^(N/2): its square is -1
+            const u64 w = tw[2];
             if (w * w % p != p - 1) return "psi^(N/2) squared is not -1";
         }
+        for (u32 k = 0; k < P.N; k += 1 + P.N / 64)  // Shoup companions
+            if (tw[2 * k] >= p || tw[2 * k + 1] != (u32)(((u64)tw[2 * k] << 32) / p)) return "bad Shoup twiddle";
         M = mul_small(M, p);
     }
     if (bitlen(M) - 1 < 2 * (int)P.W + P.logN + 3) return "M too small";

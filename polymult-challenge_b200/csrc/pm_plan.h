@@ -51,8 +51,9 @@ struct Plan {
     std::vector<uint32_t> crt_cc;     // [KP] crt_c * pinv mod 2^32 (Montgomery-Shoup companion)
     std::vector<float> rcp;           // [KP] 1/p_j (0 for padding)
 
-    // twiddles: tw[j][k] = psi_j^bitrev_logN(k) * R mod p_j, k < N
-    std::vector<uint32_t> tw;         // [K][N]
+    // twiddles in Shoup form: tw[j][k] = {w, floor(w 2^32 / p_j)}, w = psi_j^bitrev_logN(k) mod p_j,
+    // k < N (two words per entry)
+    std::vector<uint32_t> tw;         // [K][N][2]
 
     // plain (CUDA-core) GEMM tables
     int HP = 0;                       // 2L rounded up to a multiple of 4
