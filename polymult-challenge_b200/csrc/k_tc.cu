@@ -429,7 +429,7 @@ struct CrtSmem {
     unsigned char* b;
     unsigned char* a;
     uint32_t* z;
-    uint4* cst;
+    uint2* cst;
     float* spart;
     uint64_t* bars;
     uint32_t* slot;
@@ -443,7 +443,7 @@ __device__ __forceinline__ CrtSmem crt_smem(unsigned char* base, const DevPlan& 
     m.b = base;
     m.a = m.b + (size_t)P.crt_nrows * P.crt_kbytes;
     m.z = reinterpret_cast<uint32_t*>(m.a + (size_t)TC_M * P.crt_kbytes);
-    m.cst = reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(m.z) + crt_z_bytes(P));
+    m.cst = reinterpret_cast<uint2*>(reinterpret_cast<unsigned char*>(m.z) + crt_z_bytes(P));
     m.spart = reinterpret_cast<float*>(m.cst + P.KP);
     m.bars = reinterpret_cast<uint64_t*>(m.spart + 4 * TC_M);
     m.slot = reinterpret_cast<uint32_t*>(m.bars + 7);
@@ -481,8 +481,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         *S.abort = 0;
         bulk_g2s_all(S.b, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
     }
-    for (int j = threadIdx.x; j < KP; j += blockDim.x)
-        S.cst[j] = make_uint4(P.p[j], P.crt_c[j], P.crt_cc[j], __float_as_uint(P.rcp[j]));
+    for (int j = threadIdx.x; j < KP; j += blockDim.x) S.cst[j] = make_uint2(P.p[j], __float_as_uint(P.rcp[j]));
     if (warp == 0) tmem_alloc(S.slot, 2 * AS);
     tc_fence_before();
     __syncthreads();
@@ -494,8 +493,10 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     if (threadIdx.x < CRT_PROD_THREADS) {
         // ---------------- producers ----------------
         // thread (m, h): position m of the tile, groups [g0, g0 + ng) of 4 primes (half h of
-        // the G = KP / 4 groups; the padding primes K..KP-1 have zero constants, so they add
-        // nothing to A's product with the zero B columns nor to the partial sums)
+        // the G = KP / 4 groups).  The residues arrive as y_j itself in [0, 2p_j): the operand
+        // whose transform the fused row pass reads was decomposed with every constant times
+        // gamma_j = crt_c_j 2^-32, the CRT's per-prime factor.  The padding primes K..KP-1 meet
+        // zero B columns (but for A's v column, written after them) and have 1/p = 0.
         const int m = threadIdx.x & (TC_M - 1), h = threadIdx.x >> 7;
         const int G = KP / 4;
         const int gh = (G + 1) / 2;
@@ -538,9 +539,9 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                     uint32_t yy[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const uint4 c = S.cst[4 * g + q];
-                        yy[q] = red_once(mul_ms(x[4 * gl + q], c.y, c.z, c.x), c.x);
-                        s4[q] = fmaf((float)yy[q], __uint_as_float(c.w), s4[q]);
+                        const uint2 c = S.cst[4 * g + q];
+                        yy[q] = red_once(x[4 * gl + q], c.x);
+                        s4[q] = fmaf((float)yy[q], __uint_as_float(c.y), s4[q]);
                     }
                     *reinterpret_cast<uint4*>(arow + (size_t)g * 128) = make_uint4(yy[0], yy[1], yy[2], yy[3]);
                 }
@@ -561,6 +562,17 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             // acc_empty[b] after that)
             if (i > 1) wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
             S.spart[(b * 2 + h) * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            if (part.mode == CRT_FULL) {
+                // v = round(sum y_j / p_j) (|x| < M/8 keeps the sum within 1/8 of an integer;
+                // further than 1/4 is a failed check) into A's v column: the MMA adds v T_1
+                named_sync(1, CRT_PROD_THREADS);
+                if (h == 0) {
+                    const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
+                    const float vf = rintf(sum);
+                    if ((uint32_t)m < npos - pos0 && fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
+                    arow[(size_t)(P.crt_kv >> 4) * 128 + (P.crt_kv & 15)] = (unsigned char)min(max((int)vf, 0), K);
+                }
+            }
             fence_smem_to_async();
             named_sync(1, CRT_PROD_THREADS);
             if (threadIdx.x == 0) {
@@ -595,18 +607,15 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             const bool got = __all_sync(0xffffffffu, wait_or_abort(v_ready + b, (i >> 1) & 1, S.abort) &&
                                                          wait_or_abort(mma_done + b, (i >> 1) & 1, S.abort));
             tc_fence_after();
-            const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
-            const float vf = rintf(sum);
-            if (part.mode == CRT_FULL && hf == 0 && valid && got && fabsf(sum - vf) > 0.25f)
-                flag_error(P.status, DEV_ERR_CRT_BOUND);
-            const int v = part.mode == CRT_FULL ? min(max((int)vf, 0), K) : 0;
             const size_t gpos = (size_t)bt * npos + pos0;  // first coefficient of the tile in the partial buffers
-            if (part.mode != CRT_FULL && part.add_s && hf == 0 && valid)
+            if (part.mode != CRT_FULL && part.add_s && hf == 0 && valid) {
+                const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
                 part.sp[gpos + m] = (part.mode == CRT_PARTIAL_FIRST ? 0.f : part.sp[gpos + m]) + sum;
-            // accumulator bytes -> limbs with carries, + v T_1 (T_1 = (-M) mod q; v T_1 == T_v mod q,
-            // < 2^(W+7), and the fold below reduces it; one row for every lane instead of a
-            // per-lane row T_v); half hf owns limbs [0, lh) or [lh, zl)
-            const uint32_t* T1 = P.tneg + L;
+            }
+            // accumulator bytes -> limbs with carries (the MMA already added v T_1: T_1 = (-M) mod q,
+            // v T_1 == T_v mod q, < 2^(W+7), and the fold below reduces it); half hf owns limbs
+            // [0, lh) or [lh, zl).  Byte sums are < 2^25: r0 + r1 2^8 and r2 + r3 2^8 each take one
+            // wide multiply-add.
             const uint32_t tacc = tmem + (uint32_t)b * AS + ((uint32_t)((warp & 3) * 32) << 16);
             uint64_t carry = 0;
             const int c0 = hf ? lh / 4 : 0, c1 = hf ? nl / 4 : lh / 4;
@@ -628,9 +637,9 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                     if (u == 1 && !two) break;
 #pragma unroll
                     for (int q = 0; q < 4; ++q, ++l) {
-                        const uint64_t t = carry + (uint64_t)r[u][4 * q] + ((uint64_t)r[u][4 * q + 1] << 8) +
-                                           ((uint64_t)r[u][4 * q + 2] << 16) + ((uint64_t)r[u][4 * q + 3] << 24) +
-                                           (l < L ? (uint64_t)(uint32_t)v * __ldg(T1 + l) : 0ull);
+                        const uint64_t lo = (uint64_t)r[u][4 * q] + (uint64_t)r[u][4 * q + 1] * 256u;
+                        const uint64_t hi = (uint64_t)r[u][4 * q + 2] + (uint64_t)r[u][4 * q + 3] * 256u;
+                        const uint64_t t = carry + lo + (hi << 16);
                         if (l < zl) z[l] = (uint32_t)t;
                         carry = t >> 32;
                     }
@@ -689,18 +698,44 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 continue;
             }
             // coalesced store of the tile's cnt x L limbs (contiguous in the output); element w =
-            // row mm, limb col is tracked incrementally (w advances by 256 = qL rows + rL limbs)
+            // row mm, limb col, tracked incrementally (each sweep advances w by qL rows + rL
+            // limbs).  With a 16-byte aligned run, 4 consecutive words per thread and sweep.
             uint32_t* o = out + ((size_t)bt * npos + pos0) * L;
             const int tot = cnt * L;
-            const int qL = CRT_EPI_THREADS / L, rL = CRT_EPI_THREADS - qL * L;
-            int mm = et / L, col = et - mm * L;
-            for (int w = et; w < tot; w += CRT_EPI_THREADS) {
-                o[w] = S.z[(size_t)mm * zs + col];
-                mm += qL;
-                col += rL;
-                if (col >= L) {
-                    col -= L;
-                    ++mm;
+            if (((uintptr_t)o & 15) == 0 && (tot & 3) == 0) {
+                constexpr int step = 4 * CRT_EPI_THREADS;
+                const int qL = step / L, rL = step - qL * L;
+                int mm = (4 * et) / L, col = 4 * et - mm * L;
+                for (int w = 4 * et; w < tot; w += step) {
+                    uint32_t v4[4];
+                    int m2 = mm, c2 = col;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        v4[k] = S.z[(size_t)m2 * zs + c2];
+                        if (++c2 == L) {
+                            c2 = 0;
+                            ++m2;
+                        }
+                    }
+                    *reinterpret_cast<uint4*>(o + w) = make_uint4(v4[0], v4[1], v4[2], v4[3]);
+                    mm += qL;
+                    col += rL;
+                    if (col >= L) {
+                        col -= L;
+                        ++mm;
+                    }
+                }
+            } else {
+                const int qL = CRT_EPI_THREADS / L, rL = CRT_EPI_THREADS - qL * L;
+                int mm = et / L, col = et - mm * L;
+                for (int w = et; w < tot; w += CRT_EPI_THREADS) {
+                    o[w] = S.z[(size_t)mm * zs + col];
+                    mm += qL;
+                    col += rL;
+                    if (col >= L) {
+                        col -= L;
+                        ++mm;
+                    }
                 }
             }
         }
@@ -722,7 +757,7 @@ size_t rns_tc_smem(const DevPlan& P) {
 }
 
 size_t crt_tc_smem(const DevPlan& P, bool partial) {
-    return (size_t)P.crt_nrows * P.crt_kbytes + (size_t)TC_M * P.crt_kbytes + crt_z_bytes(P) + (size_t)P.KP * 16 +
+    return (size_t)P.crt_nrows * P.crt_kbytes + (size_t)TC_M * P.crt_kbytes + crt_z_bytes(P) + (size_t)P.KP * 8 +
            4 * TC_M * 4 + 7 * 8 + 32 + (partial ? crt_z_bytes(P) : 0);
 }
 

@@ -39,7 +39,9 @@ struct DevPlan {
     const uint32_t* tneg;     // [K+1][L]
     const uint32_t* q;        // [L]
     const uint8_t* dec_b;     // tensor-core decomposition B operand (canonical image)
+    const uint8_t* dec_b_ra;  // the same, constants times gamma_j = crt_c_j 2^-32 (operand RA)
     const uint8_t* crt_b;     // tensor-core CRT B operand (canonical image)
+    int crt_kv;               // CRT K-byte column of v (B column: the bytes of T_1)
     int dec_nrows, dec_kbytes;
     int crt_nrows, crt_kbytes;
     uint32_t* status;         // device status word

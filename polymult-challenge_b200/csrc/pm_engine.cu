@@ -341,7 +341,9 @@ void Engine::upload_tables() {
     d.tneg = dev_upload(dev_allocs_, P.tneg, tb);
     d.q = dev_upload(dev_allocs_, P.q, tb);
     d.dec_b = dev_upload(dev_allocs_, P.dec_b, tb);
+    d.dec_b_ra = dev_upload(dev_allocs_, P.dec_b_ra, tb);
     d.crt_b = dev_upload(dev_allocs_, P.crt_b, tb);
+    d.crt_kv = P.crt_kv;
     d.dec_nrows = P.dec_gemm.n_rows;
     d.dec_kbytes = P.dec_gemm.k_bytes;
     d.crt_nrows = P.crt_gemm.n_rows;
@@ -549,6 +551,7 @@ bool Engine::make_dec_blocks() {
         b.dp.p += j0;
         b.dp.pinv += j0;
         b.dp.dec_b += (size_t)4 * j0 * dp_.dec_kbytes;
+        b.dp.dec_b_ra += (size_t)4 * j0 * dp_.dec_kbytes;
         b.dp.dec_nrows = 4 * b.dp.KP;
         b.smem = rns_tc_smem(b.dp);
         dec_blocks_.push_back(b);
@@ -581,7 +584,8 @@ bool Engine::make_crt_blocks() {
             for (int v = 0; v < nr; ++v)
                 for (int kbyte = 0; kbyte < 4 * kp; ++kbyte) {
                     const int fk = 4 * j0 + kbyte;
-                    if (fk < kb_full)
+                    // (not the v column: the blocks' partial integers leave v T_1 to k_crt_finish)
+                    if (fk < kb_full && fk != plan_.crt_kv)
                         img[umma_kmajor_offset(v, kbyte, kb)] = plan_.crt_b[umma_kmajor_offset(v0 + v, fk, kb_full)];
                 }
             CrtBlock b;
@@ -636,15 +640,21 @@ ChunkMap Engine::chunk_map(Chunk ch) const {
 // ---------------------------------------------------------------------------------------
 // launches
 // ---------------------------------------------------------------------------------------
-void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s) const {
+// ra: src is the operand whose transform the fused row pass reads (RA).  In the tensor form its
+// residues are decomposed times gamma_j, the tcgen05 CRT's per-prime factor (dec_b_ra), so that
+// the inverse transform delivers the CRT's y_j directly.
+void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s, bool ra) const {
     const uint32_t npos = plan_.nrows * ch.cw;
     if (dec_tc_) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         const int bulk = ((uintptr_t)src % 16 == 0) && ((size_t)npos * plan_.L * 4) % 16 == 0;
+        const bool scaled = ra && (crt_tc_ || crt_blocked_);
         for (const DecBlock& b : dec_blocks_) {
-            k_rns_tc<<<grid, RNS_TC_THREADS, b.smem, s>>>(b.dp, src, chunk_map(ch), npos, nb,
-                                                            R + (size_t)b.j0 * plan_.N, bulk);
+            DevPlan d = b.dp;
+            if (scaled) d.dec_b = d.dec_b_ra;
+            k_rns_tc<<<grid, RNS_TC_THREADS, b.smem, s>>>(d, src, chunk_map(ch), npos, nb, R + (size_t)b.j0 * plan_.N,
+                                                            bulk);
             cuda_check(cudaGetLastError(), "launch k_rns_tc");
         }
     } else {
@@ -715,7 +725,7 @@ void Engine::run_device(const uint32_t* a, const uint32_t* b, uint32_t* c, uint3
         const uint32_t nb = std::min(g, count - i);
         const uint32_t* ai = a + (size_t)i * cw;
         const uint32_t* bi = b + (size_t)i * cw;
-        launch_dec(ai, all, nb, d_ra_, s);
+        launch_dec(ai, all, nb, d_ra_, s, true);
         launch_cols(false, d_ra_, all, nb, s);
         launch_rows(false, d_ra_, nullptr, nb, s);
         launch_dec(bi, all, nb, d_rb_, s);
@@ -741,7 +751,7 @@ void Engine::time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint
     try {
         for (int r = 0; r < reps; ++r) {
             cuda_check(cudaEventRecord(ev[0], s), "record");
-            launch_dec(a, all, count, d_ra_, s);
+            launch_dec(a, all, count, d_ra_, s, true);
             cuda_check(cudaEventRecord(ev[1], s), "record");
             launch_cols(false, d_ra_, all, count, s);
             cuda_check(cudaEventRecord(ev[2], s), "record");
@@ -784,7 +794,7 @@ void Engine::run_group(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32
                        cudaStream_t s) const {
     if (nb == 0) return;
     const Chunk all{0, plan_.ncols};
-    launch_dec(a, all, nb, ra, s);
+    launch_dec(a, all, nb, ra, s, true);
     launch_cols(false, ra, all, nb, s);
     launch_rows(false, ra, nullptr, nb, s);
     launch_dec(b, all, nb, rb, s);
@@ -901,7 +911,7 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         cuda_check(cudaEventRecord(ev_in_[i], s_h2d_), "record");
         mark("h2d" + std::to_string(i), s_h2d_);
         cuda_check(cudaStreamWaitEvent(sc, ev_in_[i], 0), "wait");
-        launch_dec(d_in_[P] + off, ch, 1, dR[P], sc);
+        launch_dec(d_in_[P] + off, ch, 1, dR[P], sc, P == 0);
         launch_cols(false, dR[P], ch, 1, sc);
         cuda_check(cudaEventRecord(ev_done_in_[i], sc), "record");
         mark("in" + std::to_string(i), sc);

@@ -125,7 +125,8 @@ class Engine {
     const std::vector<Chunk>& out_chunks(int kind = 0) const { return cout_[kind]; }
 
     // launch helpers (also used by the tests' stage-by-stage checks)
-    void launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s) const;
+    // ra: src is the operand whose transform the fused row pass reads (RA); see pm_engine.cu
+    void launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s, bool ra = false) const;
     void launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s) const;
     void launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s,
                      const uint32_t* ra_sel = nullptr) const;

@@ -301,16 +301,30 @@ Plan make_plan(uint32_t N, uint32_t W, uint32_t L, const uint32_t* qlimbs) {
     P.dec_gemm.n_rows = 4 * KP;
     P.dec_gemm.k_bytes = round_up(4 * (int)L, 32);
     P.dec_b.assign(P.dec_gemm.b_bytes(), 0);
-    for (int s = 0; s < 4 * (int)L; ++s)
-        for (int j = 0; j < K; ++j) {
+    P.dec_b_ra.assign(P.dec_gemm.b_bytes(), 0);
+    for (int j = 0; j < K; ++j) {
+        // gamma_j = crt_c_j 2^-32 mod p_j: the factor the CRT applies to every residue x_j of the
+        // inverse transform (y_j = x_j gamma_j).  The transform is linear over Z_p, so scaling one
+        // operand's residues by gamma_j makes the inverse transform deliver y_j itself; dec_b_ra
+        // decomposes the operand whose transform the fused row pass reads (RA) that way.
+        const u64 p = primes[j];
+        const u64 gamma = (u64)P.crt_c[j] * powmod((1ull << 32) % p, p - 2, p) % p;
+        for (int s = 0; s < 4 * (int)L; ++s) {
             const u32 c = powmod(2, 8ull * s + 32, primes[j]);
-            for (int t = 0; t < 4; ++t)
+            const u32 cg = (u32)((u64)c * gamma % p);
+            for (int t = 0; t < 4; ++t) {
                 P.dec_b[umma_kmajor_offset(4 * j + t, s, P.dec_gemm.k_bytes)] = (uint8_t)(c >> (8 * t));
+                P.dec_b_ra[umma_kmajor_offset(4 * j + t, s, P.dec_gemm.k_bytes)] = (uint8_t)(cg >> (8 * t));
+            }
         }
+    }
 
-    // tensor-core CRT operand B: row v (result byte), K-byte 4j+t -> byte (v - t) of Q_j
+    // tensor-core CRT operand B: row v (result byte), K-byte 4j+t -> byte (v - t) of Q_j; K-byte
+    // crt_kv = 4K (the first padding byte, or one past the primes) -> byte v of T_1 = (-M) mod q,
+    // against the A column that holds v (<= K < 256), so that the MMA adds v T_1 itself
     P.crt_gemm.n_rows = round_up(4 * (int)L + 3, 16);
-    P.crt_gemm.k_bytes = round_up(4 * KP, 32);
+    P.crt_kv = 4 * K;
+    P.crt_gemm.k_bytes = round_up(std::max(4 * KP, P.crt_kv + 1), 32);
     P.crt_b.assign(P.crt_gemm.b_bytes(), 0);
     for (int j = 0; j < K; ++j)
         for (int t = 0; t < 4; ++t)
@@ -319,6 +333,9 @@ Plan make_plan(uint32_t N, uint32_t W, uint32_t L, const uint32_t* qlimbs) {
                 const uint8_t qb8 = (uint8_t)(Q[j][byte / 4] >> (8 * (byte % 4)));
                 P.crt_b[umma_kmajor_offset(v, 4 * j + t, P.crt_gemm.k_bytes)] = qb8;
             }
+    for (int v = 0; v < 4 * (int)L; ++v)
+        P.crt_b[umma_kmajor_offset(v, P.crt_kv, P.crt_gemm.k_bytes)] =
+            (uint8_t)(P.tneg[(size_t)L + v / 4] >> (8 * (v % 4)));
     return P;
 }
 

@@ -65,7 +65,9 @@ struct Plan {
     GemmShape dec_gemm;               // rows (j,t) = 4j+t, K = coefficient bytes
     GemmShape crt_gemm;               // rows = result byte v, K = (j,t) = 4j+t
     std::vector<uint8_t> dec_b;       // dec_gemm.b_bytes()
+    std::vector<uint8_t> dec_b_ra;    // dec_b with every constant times gamma_j = crt_c_j 2^-32 mod p_j
     std::vector<uint8_t> crt_b;       // crt_gemm.b_bytes()
+    int crt_kv = 0;                   // CRT K-byte column of v (its B column: the bytes of T_1)
 
     size_t coeff_words() const { return (size_t)N * L; }
     size_t residue_words() const { return (size_t)K * N; }

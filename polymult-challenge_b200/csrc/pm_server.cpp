@@ -76,7 +76,7 @@ Server::Server(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const uint
             cuda_check(cudaMemcpyAsync(s0.in, resident + (size_t)k * cw, cw * 4, cudaMemcpyHostToDevice, s0.stream),
                        "resident upload");
             uint32_t* rk = resident_ + (size_t)k * rw;
-            eng_->launch_dec(s0.in, all, 1, rk, s0.stream);
+            eng_->launch_dec(s0.in, all, 1, rk, s0.stream, /*ra=*/true);  // the fused pass's RA operand
             eng_->launch_cols(false, rk, all, 1, s0.stream);
             eng_->launch_rows(false, rk, nullptr, 1, s0.stream);
             cuda_check(cudaStreamSynchronize(s0.stream), "resident transform");
