@@ -209,10 +209,10 @@ typedef struct pm_pipeline_info {
 #define PM_PIPELINE_PINNED 1
 
 /* No reference counterpart: the autotuner of the host pipeline.  Runs `reps` pm_run calls (plus
- * a warm-up) for every schedule with body divisors in {4, 8, 16} x {4, 8, 16} on pageable (or,
- * with PM_PIPELINE_PINNED, page-locked) timing buffers, keeps the one with the lowest median wall
- * time for that kind of call, and describes it in *out.  Synchronous; about 10 x (reps + 1)
- * calls. */
+ * a warm-up) for every schedule with body divisors in {4, 8, 16} x {4, 8, 16} on pageable
+ * timing buffers (with PM_PIPELINE_PINNED: {2, 4, 8, 16} x {2, 4, 8, 16} on page-locked ones),
+ * keeps the one with the lowest median wall time for that kind of call, and describes it in *out.
+ * Synchronous; about 10 (PM_PIPELINE_PINNED: 17) x (reps + 1) calls. */
 int pm_tune_pipeline(pm_context* ctx, int reps, int flags, pm_pipeline_info* out);
 int pm_get_pipeline(const pm_context* ctx, int flags, pm_pipeline_info* out);
 

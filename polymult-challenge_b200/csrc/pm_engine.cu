@@ -461,11 +461,14 @@ double Engine::tune_host_pipeline(int reps, int kind) {
     for (size_t i = 0; i < words; ++i) a[i] = (i % plan_.L == plan_.L - 1) ? 0u : (uint32_t)(i * 2654435761u);
     double best = 1e30;
     uint32_t bi = in_body_[kind], bo = out_body_[kind];
-    const uint32_t cand[3] = {4, 8, 16};
+    // body divisors: 4, 8, 16; direct-copy calls also 2 (fewer copies, each ~4 us of DMA set-up,
+    // against more compute exposed after the last input chunk and before the first output one)
+    const uint32_t cand[4] = {2, 4, 8, 16};
     try {
         for (uint32_t ib : cand)
             for (uint32_t ob : cand) {
                 if (ib > plan_.ncols || ob > plan_.ncols) continue;
+                if (kind == 0 && (ib == 2 || ob == 2)) continue;
                 set_chunk_schedule(ib, ob, kind);
                 run_host(a, a, c);
                 std::vector<double> t;
