@@ -938,8 +938,12 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     for (size_t oc = 0; oc < cout.size(); ++oc) {
         const Chunk ch = cout[oc];
         const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
-        cudaStream_t sc = s_comp_[oc % 3];
-        if (oc % 3 != 0) cuda_check(cudaStreamWaitEvent(sc, ev_fused_, 0), "wait");
+        // staged calls spread the output chunks over three streams; direct-copy calls run them
+        // in order on one stream: each chunk's compute is shorter than its D2H, and the first
+        // chunk, which gates the first D2H, then has the GPU to itself
+        const int si = kind == 1 ? 0 : (int)(oc % 3);
+        cudaStream_t sc = s_comp_[si];
+        if (si != 0) cuda_check(cudaStreamWaitEvent(sc, ev_fused_, 0), "wait");
         launch_cols(true, d_rb_, ch, 1, sc);
         // output chunks run on three streams: each gets its own region of the partial buffers
         launch_crt(d_rb_, ch, 1, d_out_ + off, sc, (size_t)ch.col0 * nrows);

@@ -10,7 +10,8 @@ this script runs `count` multiplies through pm_run_device and checks the device 
 Select the device-resident launch of a kernel with ncu's -k / -s (skip the warm-up launches):
     ncu --set full --clock-control none -k regex:k_crt_tc -s 20 -c 1 python .../profile_case.py
 --host H then runs H multiplies through pm_run (host operands, the chunked PCIe pipeline;
---pinned puts them in page-locked memory, which pm_run copies directly); with
+--pinned puts them in page-locked memory, which pm_run copies directly; --tune runs the
+chunk-schedule autotuner for that kind of call first); with
 POLYMULT_PROFILE=1 in the environment each call prints its host and device timeline.
 """
 import argparse
@@ -28,6 +29,7 @@ def main():
     ap.add_argument("--count", type=int, default=1)
     ap.add_argument("--host", type=int, default=0)
     ap.add_argument("--pinned", action="store_true", help="host operands and result in page-locked memory")
+    ap.add_argument("--tune", action="store_true", help="tune the host pipeline's chunk schedule first")
     a = ap.parse_args()
     import numpy as np
     import torch
@@ -44,6 +46,8 @@ def main():
         m.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), a.count,
                           torch.cuda.current_stream().cuda_stream)
         m.sync()
+        if a.host and a.tune:
+            print("schedule", m.tune_pipeline(3, pinned=a.pinned))
         if a.host:
             if a.pinned:
                 def buf():
