@@ -200,10 +200,11 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
 //     re-lays the tile out as the K-major A operand once the previous tile's MMAs have read
 //     A; thread 0 then issues the MMAs of the two prime halves -- half h once the epilogue
 //     has released TMEM half h -- with one commit per half (mma_done[h]);
-//   epilogue group (warps 4-19): warp w reads TMEM lane quarter w % 4 of prime half
-//     ((w - 4) / 4) % 2, the 16-column chunks of parity (w - 4) / 8, and turns four byte
-//     columns into a 64-bit sum, one REDC and a residue store; the 256 threads of a half
-//     arrive on acc_empty[h] when they have read it.
+//   epilogue group (warps 4-19): warp w reads TMEM lane quarter w % 4, the 16-column chunks
+//     congruent to (w - 4) / 4 mod 4, of prime half 0 and then of half 1, and turns four byte
+//     columns into one sum, one REDC and a residue store; all 512 threads arrive on
+//     acc_empty[h] once they have read half h, so the next tile's half-0 MMA runs while they
+//     read half 1.
 // So tile i's epilogue (the long phase) overlaps tile i+1's copy, relayout and MMAs.  Bounded
 // waits with a shared abort flag as in the CRT kernel.
 // smem: [B image][A tile][raw ring 2 x 128*L words][bars: B, raw 2, mma_done 2, acc_empty 2]
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         for (int k = 0; k < 2; ++k) {
             mbar_init(bar_raw + k, 1);
             mbar_init(mma_done + k, 1);
-            mbar_init(acc_empty + k, DEC_EPI_THREADS / 2);
+            mbar_init(acc_empty + k, DEC_EPI_THREADS);
         }
         *abort_f = 0;
         bulk_g2s_all(b_s, P.dec_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
@@ -296,19 +297,32 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
             // the previous tile's MMAs must have read A (mma_done of its last half)
             if (i > 0) wait_or_abort(mma_done + (nhalves - 1), (i - 1) & 1, abort_f);
             named_sync(1, DEC_LOAD_THREADS);  // raw tile visible to the whole group
-            // re-layout: row mm, 16-byte group g = limbs 4g..4g+3 (zero past L or past cnt)
-            for (int w = threadIdx.x; w < TC_M * groups; w += DEC_LOAD_THREADS) {
-                const int mm = w & (TC_M - 1), g = w >> 7;
-                uint4 v = make_uint4(0, 0, 0, 0);
-                if (mm < cnt) {
-                    const uint32_t* row = raw + mm * L;
+            // re-layout: thread = row mm; 16-byte group g = limbs 4g..4g+3 (zero past L or past
+            // cnt).  The full groups unpredicated and unrolled, so that several groups' loads are
+            // in flight at once (a latency chain per group otherwise: this group of 4 warps
+            // shares the SM with the 16 epilogue warps)
+            {
+                static_assert(DEC_LOAD_THREADS == TC_M, "one loader thread per tile row");
+                const int mm = threadIdx.x;
+                const uint32_t* row = raw + mm * L;
+                unsigned char* dst = a_s + (size_t)(mm >> 3) * sbo + (mm & 7) * 16;
+                const int gfull = mm < cnt ? L / 4 : 0;
+                int g = 0;
+#pragma unroll 4
+                for (; g < gfull; ++g)
+                    *reinterpret_cast<uint4*>(dst + (size_t)g * 128) =
+                        make_uint4(row[4 * g], row[4 * g + 1], row[4 * g + 2], row[4 * g + 3]);
+                for (; g < groups; ++g) {
                     const int l0 = 4 * g;
-                    v.x = l0 < L ? row[l0] : 0u;
-                    v.y = l0 + 1 < L ? row[l0 + 1] : 0u;
-                    v.z = l0 + 2 < L ? row[l0 + 2] : 0u;
-                    v.w = l0 + 3 < L ? row[l0 + 3] : 0u;
+                    uint4 v = make_uint4(0, 0, 0, 0);
+                    if (mm < cnt) {
+                        v.x = l0 < L ? row[l0] : 0u;
+                        v.y = l0 + 1 < L ? row[l0 + 1] : 0u;
+                        v.z = l0 + 2 < L ? row[l0 + 2] : 0u;
+                        v.w = l0 + 3 < L ? row[l0 + 3] : 0u;
+                    }
+                    *reinterpret_cast<uint4*>(dst + (size_t)g * 128) = v;
                 }
-                *reinterpret_cast<uint4*>(a_s + (size_t)(mm >> 3) * sbo + (size_t)g * 128 + (mm & 7) * 16) = v;
             }
             fence_smem_to_async();
             named_sync(1, DEC_LOAD_THREADS);
@@ -341,69 +355,72 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         // r0 + r1 2^8 and r2 + r3 2^8 stay below 2^32 and x is formed in 32-bit halves
         const bool small_k = kb <= 256;
         const int we = warp - DEC_LOAD_THREADS / 32;
-        const int half = (we >> 2) & 1, sub = we >> 3, m = (warp & 3) * 32 + lane;
-        const bool active = half < nhalves;
+        const int sub = we >> 2, m = (warp & 3) * 32 + lane;  // sub 0..3: chunk residue mod 4
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(2, DEC_EPI_THREADS, *abort_f != 0)) break;
-            if (!active) continue;
             int cnt;
             (void)tile_src(tile, &cnt);
-            // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
-            const bool got = __all_sync(0xffffffffu, wait_or_abort(mma_done + half, i & 1, abort_f));
-            tc_fence_after();
             const uint32_t b = tile / tiles_per_batch;
             const uint32_t pos0 = (tile - b * tiles_per_batch) * TC_M;
             const uint32_t n = m < cnt ? chunk_pos_to_n(P, C, pos0 + m) : 0;
             uint32_t* Rb = R + (size_t)b * P.Kr * P.N + n;
-            const int j0 = half ? KH : 0;
-            const int cols = half ? n1 : n0;
-            const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
-            // this thread's 16-column chunks c16 = sub, sub + 2, ...: two TMEM loads in flight per
-            // wait, the chunks' prime constants read from shared memory while they are in flight
-            const int nch = cols / 16;
             const bool st = m < cnt;
-            for (int c16 = sub; c16 < nch && got; c16 += 4) {
-                uint32_t r[2][16];
-                uint2 pc[2][4];
-                const bool two = c16 + 2 < nch;
-                // (the second chunk's constants only if it exists: past the last chunk of half 1
-                // the index would leave the table)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    pc[0][q] = pc_s[j0 + 4 * c16 + q];
-                    pc[1][q] = two ? pc_s[j0 + 4 * (c16 + 2) + q] : make_uint2(0u, 0u);
-                }
-                tmem_ld16_async(tcol + (uint32_t)(16 * c16), r[0]);
-                if (two) tmem_ld16_async(tcol + (uint32_t)(16 * (c16 + 2)), r[1]);
-                tmem_wait_ld();
-#pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    if (u == 1 && !two) break;
-                    const int jb = j0 + 4 * (c16 + 2 * u);
-                    uint32_t* out = Rb + (size_t)jb * P.N;
+            // every epilogue warp takes half 0, then half 1: the next tile's half-0 MMA runs while
+            // half 1 is read out
+            for (int half = 0; half < nhalves; ++half) {
+                // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
+                const bool got = __all_sync(0xffffffffu, wait_or_abort(mma_done + half, i & 1, abort_f));
+                tc_fence_after();
+                const int j0 = half ? KH : 0;
+                const int cols = half ? n1 : n0;
+                const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
+                // this thread's 16-column chunks c16 = sub, sub + 4, ...: two TMEM loads in flight per
+                // wait (c16 and c16 + 4), the chunks' prime constants read from shared memory while
+                // they are in flight
+                const int nch = cols / 16;
+                for (int c16 = sub; c16 < nch && got; c16 += 8) {
+                    uint32_t r[2][16];
+                    uint2 pc[2][4];
+                    const bool two = c16 + 4 < nch;
+                    // (the second chunk's constants only if it exists: past the last chunk of half 1
+                    // the index would leave the table)
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const uint32_t p = pc[u][q].x, pinv = pc[u][q].y;
-                        const uint32_t* rq = &r[u][4 * q];
-                        uint32_t y;
-                        if (small_k) {
-                            // x = t0 + t1 2^16 with t0 = r0 + r1 2^8, t1 = r2 + r3 2^8 < 2^32
-                            const uint32_t t0 = rq[0] + (rq[1] << 8), t1 = rq[2] + (rq[3] << 8);
-                            const uint32_t lo = t0 + (t1 << 16);
-                            const uint32_t hi = (t1 >> 16) + (lo < t0 ? 1u : 0u);
-                            y = red_once(hi - __umulhi(lo * pinv, p) + p, p);
-                        } else {
-                            const uint64_t x = (uint64_t)rq[0] + ((uint64_t)rq[1] << 8) + ((uint64_t)rq[2] << 16) +
-                                               ((uint64_t)rq[3] << 24);
-                            y = red_once(redc64(x, p, pinv), p);
+                        pc[0][q] = pc_s[j0 + 4 * c16 + q];
+                        pc[1][q] = two ? pc_s[j0 + 4 * (c16 + 4) + q] : make_uint2(0u, 0u);
+                    }
+                    tmem_ld16_async(tcol + (uint32_t)(16 * c16), r[0]);
+                    if (two) tmem_ld16_async(tcol + (uint32_t)(16 * (c16 + 4)), r[1]);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        if (u == 1 && !two) break;
+                        const int jb = j0 + 4 * (c16 + 4 * u);
+                        uint32_t* out = Rb + (size_t)jb * P.N;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const uint32_t p = pc[u][q].x, pinv = pc[u][q].y;
+                            const uint32_t* rq = &r[u][4 * q];
+                            uint32_t y;
+                            if (small_k) {
+                                // x = t0 + t1 2^16 with t0 = r0 + r1 2^8, t1 = r2 + r3 2^8 < 2^32
+                                const uint32_t t0 = rq[0] + (rq[1] << 8), t1 = rq[2] + (rq[3] << 8);
+                                const uint32_t lo = t0 + (t1 << 16);
+                                const uint32_t hi = (t1 >> 16) + (lo < t0 ? 1u : 0u);
+                                y = red_once(hi - __umulhi(lo * pinv, p) + p, p);
+                            } else {
+                                const uint64_t x = (uint64_t)rq[0] + ((uint64_t)rq[1] << 8) + ((uint64_t)rq[2] << 16) +
+                                                   ((uint64_t)rq[3] << 24);
+                                y = red_once(redc64(x, p, pinv), p);
+                            }
+                            if (st && jb + q < P.K) out[(size_t)q * P.N] = y;
                         }
-                        if (st && jb + q < P.K) out[(size_t)q * P.N] = y;
                     }
                 }
+                tc_fence_before();
+                mbar_arrive(acc_empty + half);  // this thread has read TMEM half `half` of tile i
             }
-            tc_fence_before();
-            mbar_arrive(acc_empty + half);  // this thread has read TMEM half `half` of tile i
         }
     }
     __syncthreads();
