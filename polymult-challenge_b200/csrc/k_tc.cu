@@ -138,6 +138,13 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
 
 // TMA-engine bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16),
 // completing `bytes` transactions on `bar`.
+// 4-byte asynchronous global -> shared copy (no register staging); cp_async_wait_all waits for
+// all of this thread's.
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_addr(dst)),
@@ -440,13 +447,12 @@ namespace {
 
 constexpr int CRT_PROD_THREADS = 256;
 constexpr int CRT_EPI_THREADS = 256;
-constexpr int CRT_BATCH_GROUPS = 3;      // prime groups (4 primes each) per batch of producer loads
 
 struct CrtSmem {
     unsigned char* b;
     unsigned char* a;
     uint32_t* z;
-    uint2* cst;
+    float* rcp;
     float* spart;
     uint64_t* bars;
     uint32_t* slot;
@@ -460,8 +466,8 @@ __device__ __forceinline__ CrtSmem crt_smem(unsigned char* base, const DevPlan& 
     m.b = base;
     m.a = m.b + (size_t)P.crt_nrows * P.crt_kbytes;
     m.z = reinterpret_cast<uint32_t*>(m.a + (size_t)TC_M * P.crt_kbytes);
-    m.cst = reinterpret_cast<uint2*>(reinterpret_cast<unsigned char*>(m.z) + crt_z_bytes(P));
-    m.spart = reinterpret_cast<float*>(m.cst + P.KP);
+    m.rcp = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(m.z) + crt_z_bytes(P));
+    m.spart = m.rcp + P.KP;
     m.bars = reinterpret_cast<uint64_t*>(m.spart + 4 * TC_M);
     m.slot = reinterpret_cast<uint32_t*>(m.bars + 7);
     m.abort = reinterpret_cast<volatile int*>(m.slot + 1);
@@ -498,7 +504,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         *S.abort = 0;
         bulk_g2s_all(S.b, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
     }
-    for (int j = threadIdx.x; j < KP; j += blockDim.x) S.cst[j] = make_uint2(P.p[j], __float_as_uint(P.rcp[j]));
+    for (int j = threadIdx.x; j < KP; j += blockDim.x) S.rcp[j] = P.rcp[j];
     if (warp == 0) tmem_alloc(S.slot, 2 * AS);
     tc_fence_before();
     __syncthreads();
@@ -510,10 +516,14 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     if (threadIdx.x < CRT_PROD_THREADS) {
         // ---------------- producers ----------------
         // thread (m, h): position m of the tile, groups [g0, g0 + ng) of 4 primes (half h of
-        // the G = KP / 4 groups).  The residues arrive as y_j itself in [0, 2p_j): the operand
-        // whose transform the fused row pass reads was decomposed with every constant times
-        // gamma_j = crt_c_j 2^-32, the CRT's per-prime factor.  The padding primes K..KP-1 meet
-        // zero B columns (but for A's v column, written after them) and have 1/p = 0.
+        // the G = KP / 4 groups).  The residues arrive as y_j itself (times a multiple of p_j):
+        // the operand whose transform the fused row pass reads was decomposed with every
+        // constant times gamma_j = crt_c_j 2^-32, the CRT's per-prime factor.  They stay
+        // unreduced in [0, 2p_j): with y'_j = y_j + d_j p_j, sum y'_j M/p_j and
+        // v' = round(sum y'_j / p_j) both grow by (sum d_j) M, so z = sum y'_j Q_j + v' T_1 is
+        // the same residue mod q, v' <= 2K - 1 <= 255 still fits A's v byte, and the fractional
+        // part of the sum, which the exactness check reads, is unchanged.  The padding primes
+        // K..KP-1 meet zero B columns (but for A's v column, written after them) and 1/p = 0.
         const int m = threadIdx.x & (TC_M - 1), h = threadIdx.x >> 7;
         const int G = KP / 4;
         const int gh = (G + 1) / 2;
@@ -530,50 +540,31 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             // partial sums only feed accumulator rows the epilogue does not store
             const uint32_t pm = (uint32_t)m < npos - pos0 ? pos0 + m : pos0;
             const uint32_t* rp = R + (size_t)bt * P.Kr * N + chunk_pos_to_n(P, C, pm) + (size_t)(4 * g0) * N;
-            // residues in batches of CRT_BATCH_GROUPS groups (4 primes each), the next batch's
-            // loads in flight while this batch is converted: up to 2 x 12 loads per thread
-            float s4[4] = {0.f, 0.f, 0.f, 0.f};
-            uint32_t xa[4 * CRT_BATCH_GROUPS], xb[4 * CRT_BATCH_GROUPS];
-            auto load_batch = [&](uint32_t(&x)[4 * CRT_BATCH_GROUPS], int bat) {
-                const uint32_t* q = rp + (size_t)(4 * CRT_BATCH_GROUPS * bat) * N;
-                // primes left from the batch's first (>= 1: its first group is this half's);
-                // slots past them re-read the last one and are not converted
-                const int left = K - 4 * (g0 + CRT_BATCH_GROUPS * bat);
-                if (left >= 4 * CRT_BATCH_GROUPS) {
-#pragma unroll
-                    for (int u = 0; u < 4 * CRT_BATCH_GROUPS; ++u) x[u] = __ldg(q + (size_t)u * N);
-                } else {
-#pragma unroll
-                    for (int u = 0; u < 4 * CRT_BATCH_GROUPS; ++u) x[u] = __ldg(q + (size_t)min(u, left - 1) * N);
-                }
-            };
-            auto convert_batch = [&](const uint32_t(&x)[4 * CRT_BATCH_GROUPS], int bat) {
-#pragma unroll
-                for (int gl = 0; gl < CRT_BATCH_GROUPS; ++gl) {
-                    const int gg = bat * CRT_BATCH_GROUPS + gl;
-                    if (gg >= ng) break;
-                    const int g = g0 + gg;
-                    uint32_t yy[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const uint2 c = S.cst[4 * g + q];
-                        yy[q] = red_once(x[4 * gl + q], c.x);
-                        s4[q] = fmaf((float)yy[q], __uint_as_float(c.y), s4[q]);
-                    }
-                    *reinterpret_cast<uint4*>(arow + (size_t)g * 128) = make_uint4(yy[0], yy[1], yy[2], yy[3]);
-                }
-            };
-            const int nbat = (ng + CRT_BATCH_GROUPS - 1) / CRT_BATCH_GROUPS;
-            load_batch(xa, 0);
             // the previous tile's MMA must have read the A tile before it is overwritten
             if (i > 0) wait_or_abort(mma_done + ((i - 1) & 1), ((i - 1) >> 1) & 1, S.abort);
-            for (int bat = 0; bat < nbat; bat += 2) {
-                if (bat + 1 < nbat) load_batch(xb, bat + 1);
-                convert_batch(xa, bat);
-                if (bat + 1 < nbat) {
-                    if (bat + 2 < nbat) load_batch(xa, bat + 2);
-                    convert_batch(xb, bat + 1);
-                }
+            // every residue of this thread's primes straight into its A row with 4-byte async
+            // copies: no register staging, the whole tile in flight at once (register batches
+            // held ~24 KB per SM in flight and left the loads latency-bound); prime slots past K
+            // re-read prime K-1
+#pragma unroll 2
+            for (int gg = 0; gg < ng; ++gg) {
+                const int g = g0 + gg;
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    cp_async4(arow + (size_t)g * 128 + 4 * k, rp + (size_t)(min(4 * g + k, K - 1) - 4 * g0) * N);
+            }
+            cp_async_wait_all();
+            // sum y'_j / p_j over this thread's primes, read back from its A row
+            float s4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+            for (int gg = 0; gg < ng; ++gg) {
+                const int g = g0 + gg;
+                const uint4 x = *reinterpret_cast<const uint4*>(arow + (size_t)g * 128);
+                const float4 r = *reinterpret_cast<const float4*>(S.rcp + 4 * g);
+                s4[0] = fmaf((float)x.x, r.x, s4[0]);
+                s4[1] = fmaf((float)x.y, r.y, s4[1]);
+                s4[2] = fmaf((float)x.z, r.z, s4[2]);
+                s4[3] = fmaf((float)x.w, r.w, s4[3]);
             }
             // the epilogue of tile i - 2 must have read partial sums [b] (it arrives on
             // acc_empty[b] after that)
@@ -587,7 +578,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                     const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
                     const float vf = rintf(sum);
                     if ((uint32_t)m < npos - pos0 && fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
-                    arow[(size_t)(P.crt_kv >> 4) * 128 + (P.crt_kv & 15)] = (unsigned char)min(max((int)vf, 0), K);
+                    arow[(size_t)(P.crt_kv >> 4) * 128 + (P.crt_kv & 15)] = (unsigned char)min(max((int)vf, 0), 2 * K - 1);
                 }
             }
             fence_smem_to_async();
@@ -774,7 +765,7 @@ size_t rns_tc_smem(const DevPlan& P) {
 }
 
 size_t crt_tc_smem(const DevPlan& P, bool partial) {
-    return (size_t)P.crt_nrows * P.crt_kbytes + (size_t)TC_M * P.crt_kbytes + crt_z_bytes(P) + (size_t)P.KP * 8 +
+    return (size_t)P.crt_nrows * P.crt_kbytes + (size_t)TC_M * P.crt_kbytes + crt_z_bytes(P) + (size_t)P.KP * 4 +
            4 * TC_M * 4 + 7 * 8 + 32 + (partial ? crt_z_bytes(P) : 0);
 }
 
@@ -800,7 +791,7 @@ __global__ void __launch_bounds__(TC_M) k_crt_finish(DevPlan P, const uint32_t* 
         const float sum = sp[c0 + m];
         const float vf = rintf(sum);
         if (fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
-        const uint32_t v = (uint32_t)min(max((int)vf, 0), P.K);
+        const uint32_t v = (uint32_t)min(max((int)vf, 0), 2 * P.K);  // residues unreduced: v < 2K
         uint32_t* z = zrow + (size_t)m * zs;
         const uint32_t* T1 = P.tneg + L;
         uint64_t carry = 0;
