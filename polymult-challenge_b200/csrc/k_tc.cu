@@ -410,16 +410,17 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                             const uint32_t p = pc[u][q].x, pinv = pc[u][q].y;
                             const uint32_t* rq = &r[u][4 * q];
                             uint32_t y;
+                            // residue = REDC(x) in (0, 2p), stored unreduced: it only feeds the forward transform,
+                            // whose Harvey butterflies take inputs below 4p
                             if (small_k) {
-                                // x = t0 + t1 2^16 with t0 = r0 + r1 2^8, t1 = r2 + r3 2^8 < 2^32
+                                // x = t0 + t1 2^16 (one wide multiply-add) with t0 = r0 + r1 2^8 and t1 = r2 + r3 2^8
+                                // below 2^32
                                 const uint32_t t0 = rq[0] + (rq[1] << 8), t1 = rq[2] + (rq[3] << 8);
-                                const uint32_t lo = t0 + (t1 << 16);
-                                const uint32_t hi = (t1 >> 16) + (lo < t0 ? 1u : 0u);
-                                y = red_once(hi - __umulhi(lo * pinv, p) + p, p);
+                                y = redc64((uint64_t)t1 * 65536u + t0, p, pinv);
                             } else {
                                 const uint64_t x = (uint64_t)rq[0] + ((uint64_t)rq[1] << 8) + ((uint64_t)rq[2] << 16) +
                                                    ((uint64_t)rq[3] << 24);
-                                y = red_once(redc64(x, p, pinv), p);
+                                y = redc64(x, p, pinv);
                             }
                             if (st && jb + q < P.K) out[(size_t)q * P.N] = y;
                         }
