@@ -508,8 +508,10 @@ def run_ours(args):
     tfile = os.path.join(REPO, "profiles", "traffic_bytes.json")
     if os.path.exists(tfile):
         try:
-            t1 = json.load(open(tfile)).get(info["gemm"], {}).get(dom)
-            traffic = None if t1 is None else t1 * B  # captured on one multiply; scales with the count
+            tt = json.load(open(tfile)).get(info["gemm"], {})
+            t1 = tt.get(dom)
+            # captured on launches of tt["multiplies_per_launch"] multiplies; scaled to B
+            traffic = None if t1 is None else int(t1 * B / tt.get("multiplies_per_launch", 1))
         except Exception:
             traffic = None
     roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
