@@ -218,7 +218,9 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
 //       [slot][abort][{p, p^-1 mod 2^32} x KP]
 // ----------------------------------------------------------------------------------------
 constexpr int DEC_LOAD_THREADS = 128;
-constexpr int DEC_EPI_THREADS = 512;
+constexpr int DEC_EPI_THREADS = RNS_TC_THREADS - DEC_LOAD_THREADS;
+constexpr int DEC_SUBS = DEC_EPI_THREADS / TC_M;  // epilogue warps per TMEM lane quarter
+static_assert(DEC_EPI_THREADS % TC_M == 0, "whole warps per lane quarter");
 
 __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const uint32_t* __restrict__ src, ChunkMap C,
                                                               uint32_t npos, uint32_t nbatch, uint32_t* __restrict__ R,
@@ -362,7 +364,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         // r0 + r1 2^8 and r2 + r3 2^8 stay below 2^32 and x is formed in 32-bit halves
         const bool small_k = kb <= 256;
         const int we = warp - DEC_LOAD_THREADS / 32;
-        const int sub = we >> 2, m = (warp & 3) * 32 + lane;  // sub 0..3: chunk residue mod 4
+        const int sub = we >> 2, m = (warp & 3) * 32 + lane;  // sub < DEC_SUBS: chunk residue mod DEC_SUBS
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(2, DEC_EPI_THREADS, *abort_f != 0)) break;
@@ -382,28 +384,28 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                 const int j0 = half ? KH : 0;
                 const int cols = half ? n1 : n0;
                 const uint32_t tcol = tmem + (half ? col1 : 0) + ((uint32_t)((warp & 3) * 32) << 16);
-                // this thread's 16-column chunks c16 = sub, sub + 4, ...: two TMEM loads in flight per
-                // wait (c16 and c16 + 4), the chunks' prime constants read from shared memory while
-                // they are in flight
+                // this thread's 16-column chunks c16 = sub, sub + DEC_SUBS, ...: two TMEM loads in
+                // flight per wait (c16 and c16 + DEC_SUBS), the chunks' prime constants read from
+                // shared memory while they are in flight
                 const int nch = cols / 16;
-                for (int c16 = sub; c16 < nch && got; c16 += 8) {
+                for (int c16 = sub; c16 < nch && got; c16 += 2 * DEC_SUBS) {
                     uint32_t r[2][16];
                     uint2 pc[2][4];
-                    const bool two = c16 + 4 < nch;
+                    const bool two = c16 + DEC_SUBS < nch;
                     // (the second chunk's constants only if it exists: past the last chunk of half 1
                     // the index would leave the table)
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         pc[0][q] = pc_s[j0 + 4 * c16 + q];
-                        pc[1][q] = two ? pc_s[j0 + 4 * (c16 + 4) + q] : make_uint2(0u, 0u);
+                        pc[1][q] = two ? pc_s[j0 + 4 * (c16 + DEC_SUBS) + q] : make_uint2(0u, 0u);
                     }
                     tmem_ld16_async(tcol + (uint32_t)(16 * c16), r[0]);
-                    if (two) tmem_ld16_async(tcol + (uint32_t)(16 * (c16 + 4)), r[1]);
+                    if (two) tmem_ld16_async(tcol + (uint32_t)(16 * (c16 + DEC_SUBS)), r[1]);
                     tmem_wait_ld();
 #pragma unroll
                     for (int u = 0; u < 2; ++u) {
                         if (u == 1 && !two) break;
-                        const int jb = j0 + 4 * (c16 + 4 * u);
+                        const int jb = j0 + 4 * (c16 + DEC_SUBS * u);
                         uint32_t* out = Rb + (size_t)jb * P.N;
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
