@@ -210,9 +210,10 @@ typedef struct pm_pipeline_info {
 
 /* No reference counterpart: the autotuner of the host pipeline.  Runs `reps` pm_run calls (plus
  * a warm-up) for every schedule with body divisors in {4, 8, 16} x {4, 8, 16} on pageable
- * timing buffers (with PM_PIPELINE_PINNED: {2, 4, 8, 16} x {2, 4, 8, 16} on page-locked ones),
- * keeps the one with the lowest median wall time for that kind of call, and describes it in *out.
- * Synchronous; about 10 (PM_PIPELINE_PINNED: 17) x (reps + 1) calls. */
+ * timing buffers (with PM_PIPELINE_PINNED: {2, 3, 4, 8, 16} x {2, 3, 4, 8, 16} on page-locked
+ * ones; 3 stands for the chunks 1/2, 1/4, 1/4 of b and 1/4, 1/4, 1/2 of c), keeps the one with the
+ * lowest median wall time for that kind of call, and describes it in *out.  Synchronous; about
+ * 10 (PM_PIPELINE_PINNED: 26) x (reps + 1) calls. */
 int pm_tune_pipeline(pm_context* ctx, int reps, int flags, pm_pipeline_info* out);
 int pm_get_pipeline(const pm_context* ctx, int flags, pm_pipeline_info* out);
 

@@ -406,17 +406,21 @@ void Engine::ensure_scratch(uint32_t group) {
 // a D2H, the first output chunk's latency (inverse column pass + CRT, ~30 us at N = 65536)
 // hardly depends on its width, and each copy costs a few microseconds of DMA set-up.  Events
 // sized for the longer schedule.
+// Direct-copy calls also take divisor 3 for either side: b in [1/2, 1/4, 1/4] (the last chunk,
+// whose compute is exposed, a quarter) and the output in [1/4, 1/4, 1/2] (the first, which gates
+// the first D2H, a quarter) -- three copies each.
 void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind) {
-    if (in_body == 0 || out_body == 0 || (in_body & (in_body - 1)) || (out_body & (out_body - 1)))
-        throw InvalidPoint("chunk divisors must be powers of two");
     if (kind != 0 && kind != 1) throw InvalidPoint("pipeline kind must be 0 (staged) or 1 (direct)");
+    auto ok = [&](uint32_t d) { return d != 0 && ((d & (d - 1)) == 0 || (kind == 1 && d == 3)); };
+    if (!ok(in_body) || !ok(out_body))
+        throw InvalidPoint("chunk divisors must be powers of two (or 3 for direct-copy calls)");
     const uint32_t nc = plan_.ncols;
     if (kind == 0) {
         cin_[kind] = make_chunks(nc, {32, 32, 16}, in_body, {});
         cout_[kind] = make_chunks(nc, {64, 32}, out_body, {32, 64});
     } else {
-        cin_[kind] = make_chunks(nc, {}, in_body, {});
-        cout_[kind] = make_chunks(nc, {}, out_body, {});
+        cin_[kind] = in_body == 3 ? make_chunks(nc, {2}, 4, {}) : make_chunks(nc, {}, in_body, {});
+        cout_[kind] = out_body == 3 ? make_chunks(nc, {}, 4, {2}) : make_chunks(nc, {}, out_body, {});
     }
     in_body_[kind] = in_body;
     out_body_[kind] = out_body;
@@ -461,14 +465,15 @@ double Engine::tune_host_pipeline(int reps, int kind) {
     for (size_t i = 0; i < words; ++i) a[i] = (i % plan_.L == plan_.L - 1) ? 0u : (uint32_t)(i * 2654435761u);
     double best = 1e30;
     uint32_t bi = in_body_[kind], bo = out_body_[kind];
-    // body divisors: 4, 8, 16; direct-copy calls also 2 (fewer copies, each ~4 us of DMA set-up,
-    // against more compute exposed after the last input chunk and before the first output one)
-    const uint32_t cand[4] = {2, 4, 8, 16};
+    // body divisors: 4, 8, 16; direct-copy calls also 2 and 3 (fewer copies, each ~4 us of DMA
+    // set-up, against more compute exposed after the last input chunk and before the first output
+    // one; 3: the uneven three-chunk shapes of set_chunk_schedule)
+    const uint32_t cand[5] = {2, 3, 4, 8, 16};
     try {
         for (uint32_t ib : cand)
             for (uint32_t ob : cand) {
                 if (ib > plan_.ncols || ob > plan_.ncols) continue;
-                if (kind == 0 && (ib == 2 || ob == 2)) continue;
+                if (kind == 0 && (ib < 4 || ob < 4)) continue;
                 set_chunk_schedule(ib, ob, kind);
                 run_host(a, a, c);
                 std::vector<double> t;

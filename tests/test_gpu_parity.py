@@ -155,7 +155,7 @@ def test_tuned_pipeline_still_bit_exact():
         # the page-locked schedule is tuned on its own and leaves the staged one alone
         assert m.pipeline(pinned=True)["tuned_ms"] == 0
         pinfo = m.tune_pipeline(2, pinned=True)
-        assert pinfo["in_body"] in (2, 4, 8, 16) and pinfo["out_body"] in (2, 4, 8, 16) and pinfo["tuned_ms"] > 0
+        assert pinfo["in_body"] in (2, 3, 4, 8, 16) and pinfo["out_body"] in (2, 3, 4, 8, 16) and pinfo["tuned_ms"] > 0
         assert m.pipeline(pinned=True) == pinfo and m.pipeline() == info
         for case in pt["cases"]:
             a, b, _ = regen_case(pt, case)
