@@ -234,6 +234,13 @@ const char* pm_last_error(void);
  * Fills *K_out with the prime count.  Usable on a machine without a GPU. */
 int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int32_t* K_out);
 
+/* Host-only: stress test of the thread pool that stages pm_run's pageable operands.  Creates
+ * `pools` pools of `workers` threads and runs `runs` task sets on each (task counts 1..64,
+ * varying when `vary`, else 64 every time), counting task sets where a task ran other than once
+ * or was still running when the set returned.  *failures gets that count (0 expected).  No GPU
+ * needed. */
+int pm_selftest_host_pool(uint32_t pools, uint32_t runs, uint32_t workers, int vary, uint64_t* failures);
+
 #ifdef __cplusplus
 }
 #endif

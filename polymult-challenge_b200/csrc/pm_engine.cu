@@ -55,7 +55,8 @@ HostPool::~HostPool() {
 bool HostPool::work_once(uint64_t gen) {
     uint64_t c = claim_.load(std::memory_order_acquire);
     for (;;) {
-        if ((c >> 32) != gen || (int)(uint32_t)c >= n_.load(std::memory_order_acquire)) return false;
+        // unsigned: a closed generation's index (all ones) is past every task count
+        if ((c >> 32) != gen || (uint32_t)c >= (uint32_t)n_.load(std::memory_order_acquire)) return false;
         if (claim_.compare_exchange_weak(c, c + 1, std::memory_order_acq_rel, std::memory_order_acquire)) break;
     }
     (*fn_)((int)(uint32_t)c);
@@ -65,10 +66,15 @@ bool HostPool::work_once(uint64_t gen) {
 
 void HostPool::run(int n, const std::function<void(int)>& fn) {
     if (n <= 0) return;
+    const uint64_t prev = claim_.load(std::memory_order_relaxed) >> 32, gen = prev + 1;
+    // Close the previous generation first: its claim word gets an index no task count reaches,
+    // so a worker that read it (or the count) before this run cannot claim a task under it --
+    // its compare-exchange fails on the changed word.  Only then the task, its count and the
+    // completion counter change; the new generation's word publishes them (release).
+    claim_.store((prev << 32) | 0xFFFFFFFFull, std::memory_order_seq_cst);
     fn_ = &fn;
-    n_.store(n, std::memory_order_relaxed);
-    done_.store(0, std::memory_order_relaxed);
-    const uint64_t gen = (claim_.load(std::memory_order_relaxed) >> 32) + 1;
+    n_.store(n, std::memory_order_seq_cst);
+    done_.store(0, std::memory_order_seq_cst);
     claim_.store(gen << 32, std::memory_order_release);
     if (sleepers_.load() > 0) {
         std::lock_guard<std::mutex> lk(m_);
@@ -81,6 +87,29 @@ void HostPool::run(int n, const std::function<void(int)>& fn) {
         __builtin_ia32_pause();
 #endif
     }
+}
+
+uint64_t host_pool_selftest(uint32_t pools, uint32_t runs, int workers, bool vary) {
+    uint64_t bad = 0;
+    std::vector<std::atomic<int>> hits(64);
+    for (uint32_t pi = 0; pi < pools; ++pi) {
+        HostPool pool(workers);  // as pm_run's: workers spin between task sets
+        for (uint32_t it = 0; it < runs; ++it) {
+            const int n = vary ? 1 + (int)((it * 37u + pi) % 64u) : 64;
+            for (auto& h : hits) h.store(0, std::memory_order_relaxed);
+            std::atomic<int> inflight{0};
+            const std::function<void(int)> fn = [&](int t) {
+                inflight.fetch_add(1);
+                if (t >= 0 && t < 64) hits[t].fetch_add(1);
+                inflight.fetch_sub(1);
+            };
+            pool.run(n, fn);
+            bool ok = inflight.load() == 0;
+            for (int t = 0; t < 64 && ok; ++t) ok = hits[t].load() == (t < n ? 1 : 0);
+            if (!ok) ++bad;
+        }
+    }
+    return bad;
 }
 
 void HostPool::loop() {
@@ -102,7 +131,7 @@ void HostPool::loop() {
                 std::unique_lock<std::mutex> lk(m_);
                 cv_.wait_for(lk, std::chrono::milliseconds(100), [&] {
                     const uint64_t c = claim_.load();
-                    return stop_.load() || ((c >> 32) != gen && (int)(uint32_t)c < n_.load());
+                    return stop_.load() || ((c >> 32) != gen && (uint32_t)c < (uint32_t)n_.load());
                 });
             }
             sleepers_.fetch_sub(1);

@@ -40,6 +40,10 @@ void cuda_check(cudaError_t e, const char* what);
 // sleeping after `idle_us` without work.  Task indices are claimed with a compare-and-swap
 // on (generation << 32 | next index), so a worker still finishing an old job can never take
 // a task of the next one.
+// Stress test of HostPool::run (pm_selftest_host_pool): task sets whose tasks did not each run
+// exactly once, or were still running when run() returned.
+uint64_t host_pool_selftest(uint32_t pools, uint32_t runs, int workers, bool vary);
+
 class HostPool {
   public:
     explicit HostPool(int workers, int idle_us = 200000);

@@ -120,6 +120,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_plan_selfcheck.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, vp,
                                       ctypes.POINTER(ctypes.c_int32)]
     lib.pm_plan_selfcheck.restype = ctypes.c_int
+    lib.pm_selftest_host_pool.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_uint64)]
+    lib.pm_selftest_host_pool.restype = ctypes.c_int
     lib.pm_tune_pipeline.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
     lib.pm_tune_pipeline.restype = ctypes.c_int
     lib.pm_get_pipeline.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
@@ -164,6 +167,13 @@ def _u32(arr, shape=None) -> np.ndarray:
     if shape is not None and a.shape != shape:
         raise RuntimeError("operand size does not match N x L: got %s, want %s" % (a.shape, shape))
     return a
+
+
+def host_pool_selftest(pools: int, runs: int, workers: int = 7, vary: bool = False) -> int:
+    """Stress test of the host staging pool (pm_selftest_host_pool); returns the failures."""
+    f = ctypes.c_uint64()
+    _check(load().pm_selftest_host_pool(pools, runs, workers, 1 if vary else 0, ctypes.byref(f)))
+    return f.value
 
 
 def plan_selfcheck(N: int, W: int, q_limbs) -> int:
