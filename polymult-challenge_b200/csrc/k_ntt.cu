@@ -97,11 +97,18 @@ struct RunTw {
     }
 };
 
-// A column stage's twiddles in shared memory (Shoup form): w[m] = base[m] or, REV, base[-m].
+// A column stage's run of 2^t Shoup twiddles in shared memory, starting at `start` (aligned to
+// 2^t entries): w[m] is entry m (REV: entry 2^t - 1 - m), read as half of a 16-byte pair.
 template <bool REV>
-struct SmemTw {
-    const Tw2* base;
-    __device__ __forceinline__ Tw2 operator[](int m) const { return base[REV ? -m : m]; }
+struct SmemRun {
+    const Tw2* start;
+    int n;
+    __device__ __forceinline__ Tw2 operator[](int m) const {
+        const int e = REV ? n - 1 - m : m;
+        if (n == 1) return start[0];
+        const uint4 u = reinterpret_cast<const uint4*>(start)[e >> 1];
+        return (e & 1) ? Tw2{u.z, u.w} : Tw2{u.x, u.y};
+    }
 };
 
 // ---------------------------------------------------------------------------------------
@@ -329,14 +336,17 @@ __global__ void __launch_bounds__(128, NB >= 9 ? (FUSED ? 4 : 5) : (FUSED ? 6 : 
 // ---------------------------------------------------------------------------------------
 namespace {
 
-template <int NB, bool INV, int K>
-__device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32_t* gbase, size_t gstride, int ltc,
+// LTC >= 0: the tile width 2^LTC at compile time (shared-memory offsets become immediates);
+// -1: the runtime ltc (narrow column chunks of the host pipeline)
+template <int NB, bool INV, int K, int LTC>
+__device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32_t* gbase, size_t gstride, int ltc_rt,
                                           uint32_t p) {
     using C = LineCfg<NB>;
     constexpr int b0 = C::b0(K);
     constexpr int NGRP = (1 << NB) / C::E;  // groups per column
     constexpr bool FIRST = INV ? K == C::NPH - 1 : K == 0;
     constexpr bool LAST = INV ? K == 0 : K == C::NPH - 1;
+    const int ltc = LTC >= 0 ? LTC : ltc_rt;
     const int tc = 1 << ltc;
     const int c = threadIdx.x & (tc - 1);
     const int slots = blockDim.x >> ltc;
@@ -355,11 +365,13 @@ __device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32
 #pragma unroll
         for (int t = 0; t < C::RB; ++t)
             tb[t] = INV ? (2 << C::ls(K, t)) - 1 - (hip << t) : (1 << C::ls(K, t)) + (hip << t);
+        // stage t's 2^t twiddles: tws[tb[t] + m] (forward) or tws[tb[t] - m] (inverse), runs
+        // aligned to 2^t entries
         if (!INV) {
-            auto stw = [&](int t) { return SmemTw<false>{tws + tb[t]}; };
+            auto stw = [&](int t) { return SmemRun<false>{tws + tb[t], 1 << t}; };
             radix_fwd<C::RB, C::t0(K)>(v, stw, p);
         } else {
-            auto stw = [&](int t) { return SmemTw<true>{tws + tb[t]}; };
+            auto stw = [&](int t) { return SmemRun<true>{tws + tb[t] - ((1 << t) - 1), 1 << t}; };
             radix_inv<C::RB, C::t0(K)>(v, stw, p);
         }
 #pragma unroll
@@ -370,16 +382,16 @@ __device__ __forceinline__ void col_phase(uint32_t* tile, const Tw2* tws, uint32
     }
 }
 
-template <int NB, bool INV, int I>
+template <int NB, bool INV, int I, int LTC>
 __device__ __forceinline__ void col_phases(uint32_t* tile, const Tw2* tws, uint32_t* gbase, size_t gstride, int ltc,
                                            uint32_t p) {
     using C = LineCfg<NB>;
     if constexpr (I < C::NPH) {
         constexpr int K = INV ? C::NPH - 1 - I : I;
-        col_phase<NB, INV, K>(tile, tws, gbase, gstride, ltc, p);
+        col_phase<NB, INV, K, LTC>(tile, tws, gbase, gstride, ltc, p);
         if constexpr (I + 1 < C::NPH) {
             __syncthreads();
-            col_phases<NB, INV, I + 1>(tile, tws, gbase, gstride, ltc, p);
+            col_phases<NB, INV, I + 1, LTC>(tile, tws, gbase, gstride, ltc, p);
         }
     }
 }
@@ -387,7 +399,7 @@ __device__ __forceinline__ void col_phases(uint32_t* tile, const Tw2* tws, uint3
 }  // namespace
 
 template <int NB, bool INV>
-__global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restrict__ R, uint32_t col0, int ltc) {
+__global__ void __launch_bounds__(256, NB >= 5 ? 4 : 1) k_ntt_cols(DevPlan P, uint32_t* __restrict__ R, uint32_t col0, int ltc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NR = 1 << NB;
     Tw2* tws = reinterpret_cast<Tw2*>(smem_raw);            // [NR]
@@ -401,7 +413,8 @@ __global__ void __launch_bounds__(256) k_ntt_cols(DevPlan P, uint32_t* __restric
         tws[k] = Tw2{u.x, u.y};
     }
     __syncthreads();
-    col_phases<NB, INV, 0>(tile, tws, base, P.ncols, ltc, p);
+    if (ltc == 5) col_phases<NB, INV, 0, 5>(tile, tws, base, P.ncols, ltc, p);  // the common 32-column tile
+    else col_phases<NB, INV, 0, -1>(tile, tws, base, P.ncols, ltc, p);
 }
 
 namespace {
