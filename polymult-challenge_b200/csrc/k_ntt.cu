@@ -309,6 +309,8 @@ __global__ void __launch_bounds__(128, NB >= 9 ? (FUSED ? 4 : 5) : (FUSED ? 6 : 
     const uint2* twj = P.tw + (size_t)j * P.N;
 
     uint32_t v[C::E];
+    pdl_trigger();
+    pdl_wait();
     row_global<NB, 0, true>(v, row, r, active);
     row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p);
     if constexpr (FUSED) {
@@ -408,10 +410,12 @@ __global__ void __launch_bounds__(256, NB >= 5 ? 4 : 1) k_ntt_cols(DevPlan P, ui
     const uint32_t p = P.p[j];
     uint32_t* base = R + ((size_t)blockIdx.z * P.K + j) * P.N + col0 + ((uint32_t)blockIdx.x << ltc);
     const uint2* tw = P.tw + (size_t)j * P.N;
+    pdl_trigger();
     for (int k = threadIdx.x; k < NR; k += blockDim.x) {
         const uint2 u = __ldg(tw + k);
         tws[k] = Tw2{u.x, u.y};
     }
+    pdl_wait();
     __syncthreads();
     if (ltc == 5) col_phases<NB, INV, 0, 5>(tile, tws, base, P.ncols, ltc, p);  // the common 32-column tile
     else col_phases<NB, INV, 0, -1>(tile, tws, base, P.ncols, ltc, p);
@@ -421,16 +425,18 @@ namespace {
 
 template <int NB>
 void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
-                    int ltc) {
-    if (inv) k_ntt_cols<NB, true><<<grid, 256, smem, s>>>(P, R, col0, ltc);
-    else k_ntt_cols<NB, false><<<grid, 256, smem, s>>>(P, R, col0, ltc);
+                    int ltc, bool pdl) {
+    const cudaError_t e = launch_kernel(inv ? k_ntt_cols<NB, true> : k_ntt_cols<NB, false>, grid, dim3(256), smem, s,
+                                        pdl, P, R, col0, ltc);
+    if (e != cudaSuccess) throw_cuda(e, inv ? "launch k_ntt_cols<inverse>" : "launch k_ntt_cols<forward>");
 }
 
 template <int NB>
 void launch_rows_nb(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
-                    const uint32_t* ra_sel) {
-    if (fused) k_ntt_rows<NB, true><<<grid, 128, 0, s>>>(P, R, RA, ra_sel);
-    else k_ntt_rows<NB, false><<<grid, 128, 0, s>>>(P, R, RA, ra_sel);
+                    const uint32_t* ra_sel, bool pdl) {
+    const cudaError_t e = launch_kernel(fused ? k_ntt_rows<NB, true> : k_ntt_rows<NB, false>, grid, dim3(128), 0, s,
+                                        pdl, P, R, RA, ra_sel);
+    if (e != cudaSuccess) throw_cuda(e, fused ? "launch k_ntt_rows<fused>" : "launch k_ntt_rows<forward>");
 }
 
 // Applies F<NB>::run(...) for the line length 2^nb, nb in [0, 10].
@@ -502,13 +508,13 @@ struct RowsPerCtaF {
 }  // namespace
 
 void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
-                     int ltc) {
-    dispatch_nb<ColsF>(P.w1, inv, grid, smem, s, P, R, col0, ltc);
+                     int ltc, bool pdl) {
+    dispatch_nb<ColsF>(P.w1, inv, grid, smem, s, P, R, col0, ltc, pdl);
 }
 
 void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
-                     const uint32_t* ra_sel) {
-    dispatch_nb<RowsF>(P.w2, fused, grid, s, P, R, RA, ra_sel);
+                     const uint32_t* ra_sel, bool pdl) {
+    dispatch_nb<RowsF>(P.w2, fused, grid, s, P, R, RA, ra_sel, pdl);
 }
 
 int ntt_rows_per_cta(int w2) {

@@ -23,6 +23,8 @@ __global__ void __launch_bounds__(256) k_rns_plain(DevPlan P, const uint32_t* __
     const int cnt = (int)min((uint32_t)DEC_TM, npos - pos0);
     const uint32_t* s = src + ((size_t)b * npos + pos0) * L;
     uint32_t* Rb = R + (size_t)b * P.K * P.N;
+    pdl_trigger();
+    pdl_wait();
 
     for (int idx = threadIdx.x; idx < L * DEC_TM; idx += blockDim.x) {
         const int l = idx / DEC_TM, m = idx - l * DEC_TM;
@@ -87,6 +89,8 @@ __global__ void __launch_bounds__(128) k_crt_plain(DevPlan P, const uint32_t* __
     const uint32_t pos0 = blockIdx.x * CRT_TM;
     const int cnt = (int)min((uint32_t)CRT_TM, npos - pos0);
     const uint32_t* Rb = R + (size_t)b * K * P.N;
+    pdl_trigger();
+    pdl_wait();
 
     for (int idx = threadIdx.x; idx < KP * CRT_TM; idx += blockDim.x) {
         const int j = idx / CRT_TM, m = idx - j * CRT_TM;

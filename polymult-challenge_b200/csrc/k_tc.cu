@@ -261,21 +261,25 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         }
         *abort_f = 0;
         bulk_g2s_all(b_s, P.dec_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
-        if (use_bulk)
-            for (int k = 0; k < 2; ++k) {
-                const uint32_t t = blockIdx.x + k * gridDim.x;
-                if (t < ntiles) {
-                    int cnt;
-                    const uint32_t* s = tile_src(t, &cnt);
-                    bulk_g2s_all(raw_s + k * raw_words, s, (uint32_t)cnt * L * 4, bar_raw + k);
-                }
-            }
     }
     for (int j = threadIdx.x; j < P.KP; j += blockDim.x) pc_s[j] = make_uint2(P.p[j], P.pinv[j]);
     if (warp == 0) tmem_alloc(slot, ncols);
+    // the prologue above reads only the plan's constant tables; the operand and R come after
+    // the previous kernel in the stream
+    pdl_wait();
+    if (threadIdx.x == 0 && use_bulk)
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t t = blockIdx.x + k * gridDim.x;
+            if (t < ntiles) {
+                int cnt;
+                const uint32_t* s = tile_src(t, &cnt);
+                bulk_g2s_all(raw_s + k * raw_words, s, (uint32_t)cnt * L * 4, bar_raw + k);
+            }
+        }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    pdl_trigger();  // after this block's TMEM allocation
     const uint32_t tmem = *slot;
     // thread 0's record of what is in flight, for the abort path: the last commit (barrier and
     // phase parity) and, per ring slot, a bulk copy nobody has waited for (and its parity)
@@ -509,9 +513,13 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     }
     for (int j = threadIdx.x; j < KP; j += blockDim.x) S.rcp[j] = P.rcp[j];
     if (warp == 0) tmem_alloc(S.slot, 2 * AS);
+    // the prologue above reads only the plan's constant tables; R, the partial buffers and the
+    // output come after the previous kernel in the stream
+    pdl_wait();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    pdl_trigger();  // after this block's TMEM allocation
     const uint32_t tmem = *S.slot;
     uint32_t issued = 0;  // tiles whose MMAs thread 0 issued
     bool b_seen = false;  // thread 0 has seen the B image land
@@ -784,6 +792,8 @@ __global__ void __launch_bounds__(TC_M) k_crt_finish(DevPlan P, const uint32_t* 
     uint32_t* zrow = reinterpret_cast<uint32_t*>(smem_raw);  // [128][zs]
     const size_t c0 = (size_t)blockIdx.x * TC_M;
     const int cnt = (int)min((size_t)TC_M, total - c0);
+    pdl_trigger();
+    pdl_wait();
     for (int w = threadIdx.x; w < cnt * zl; w += TC_M) {
         const int mm = w / zl;
         zrow[(size_t)mm * zs + (w - mm * zl)] = zp[c0 * zl + w];

@@ -110,6 +110,17 @@ __device__ __forceinline__ void bfly_gs_sh(uint32_t& x, uint32_t& y, Tw2 w, uint
     y = mul_sh(d, w.w, w.wc, p);
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialization may
+// start while the kernel before it in the stream is still running.  pdl_wait() returns once
+// that kernel has completed and its memory operations are visible (at once after an ordinary
+// launch), so a kernel touches only shared memory, TMEM and the plan's constant tables before
+// it.  pdl_trigger() lets the next kernel's blocks launch, so that their prologues overlap this
+// kernel's tail; it takes effect once every block of this grid has called it or exited.
+// Kernels that allocate TMEM call it only after their own allocation: a dependent block on the
+// same SM could otherwise hold the columns while it waits for this kernel to finish.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void flag_error(uint32_t* status, uint32_t bit) {
     if (status) atomicOr(status, bit);
 }

@@ -325,7 +325,6 @@ Engine::~Engine() {
     for (auto e : ev_crt_) cudaEventDestroy(e);
     for (auto e : ev_out_) cudaEventDestroy(e);
     for (auto e : trace_ev_) cudaEventDestroy(e);
-    if (ev_row_a_) cudaEventDestroy(ev_row_a_);
     if (ev_fused_) cudaEventDestroy(ev_fused_);
     for (auto s : s_comp_)
         if (s) cudaStreamDestroy(s);
@@ -466,7 +465,7 @@ void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind) {
     mk(ev_done_in_, nin, cudaEventDisableTiming);
     mk(ev_crt_, nco, cudaEventDisableTiming);
     mk(ev_out_, nco, cudaEventDisableTiming);
-    if (profile_) mk(trace_ev_, 8 + 2 * nin + 2 * nco, cudaEventDefault);
+    if (profile_) mk(trace_ev_, 8 + 3 * nin + 3 * nco, cudaEventDefault);
 }
 
 double Engine::tune_host_pipeline(int reps, int kind) {
@@ -552,7 +551,6 @@ void Engine::setup_host_pipeline() {
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
     set_chunk_schedule(8, 8, 0);
     set_chunk_schedule(8, 8, 1);
-    cuda_check(cudaEventCreateWithFlags(&ev_row_a_, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
     // 8 copying threads (7 workers + the caller) by default.  On the 16-CPU B200 hosts measured,
     // 12 threads stage an operand pair faster in isolation (0.63 ms against 1.0 ms) but made the
@@ -680,7 +678,8 @@ ChunkMap Engine::chunk_map(Chunk ch) const {
 // ra: src is the operand whose transform the fused row pass reads (RA).  In the tensor form its
 // residues are decomposed times gamma_j, the tcgen05 CRT's per-prime factor (dec_b_ra), so that
 // the inverse transform delivers the CRT's y_j directly.
-void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s, bool ra) const {
+void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s, bool ra,
+                        bool pdl) const {
     const uint32_t npos = plan_.nrows * ch.cw;
     if (dec_tc_) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
@@ -690,41 +689,43 @@ void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R,
         for (const DecBlock& b : dec_blocks_) {
             DevPlan d = b.dp;
             if (scaled) d.dec_b = d.dec_b_ra;
-            k_rns_tc<<<grid, RNS_TC_THREADS, b.smem, s>>>(d, src, chunk_map(ch), npos, nb, R + (size_t)b.j0 * plan_.N,
-                                                            bulk);
-            cuda_check(cudaGetLastError(), "launch k_rns_tc");
+            cuda_check(launch_kernel(k_rns_tc, dim3(grid), dim3(RNS_TC_THREADS), b.smem, s, pdl, d, src,
+                                     chunk_map(ch), npos, nb, R + (size_t)b.j0 * plan_.N, bulk),
+                       "launch k_rns_tc");
+            pdl = true;  // the next prime block follows this launch
         }
     } else {
         dim3 grid((npos + DEC_TM - 1) / DEC_TM, 1, nb);
-        k_rns_plain<<<grid, 256, smem_dec_, s>>>(dp_, src, chunk_map(ch), npos, R, dec_tab_smem_ ? 1 : 0);
-        cuda_check(cudaGetLastError(), "launch k_rns_plain");
+        cuda_check(launch_kernel(k_rns_plain, grid, dim3(256), smem_dec_, s, pdl, dp_, src, chunk_map(ch), npos, R,
+                                 dec_tab_smem_ ? 1 : 0),
+                   "launch k_rns_plain");
     }
 }
 
-void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s) const {
+void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s, bool pdl) const {
     if (plan_.w1 == 0) return;
     const int ltc = ilog2(std::min<uint32_t>(32, ch.cw));
     dim3 grid(ch.cw >> ltc, plan_.K, nb);
     const size_t smem = ntt_cols_smem(dp_, ltc);
-    launch_ntt_cols(inv, grid, smem, s, dp_, R, ch.col0, ltc);
-    cuda_check(cudaGetLastError(), inv ? "launch k_ntt_cols<inverse>" : "launch k_ntt_cols<forward>");
+    launch_ntt_cols(inv, grid, smem, s, dp_, R, ch.col0, ltc, pdl);
 }
 
 void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s,
-                         const uint32_t* ra_sel) const {
+                         const uint32_t* ra_sel, bool pdl) const {
     dim3 grid((plan_.nrows + rpb_ - 1) / rpb_, plan_.K, nb);
-    launch_ntt_rows(fused, grid, s, dp_, R, RA, ra_sel);
-    cuda_check(cudaGetLastError(), fused ? "launch k_ntt_rows<fused>" : "launch k_ntt_rows<forward>");
+    launch_ntt_rows(fused, grid, s, dp_, R, RA, ra_sel, pdl);
 }
 
-void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff) const {
+void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff,
+                        bool pdl) const {
     const uint32_t npos = plan_.nrows * ch.cw;
     if (crt_tc_) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         const CrtPartial full{nullptr, nullptr, CRT_FULL, 0, 0};
-        k_crt_tc<<<grid, CRT_TC_THREADS, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, nb, out, full);
-        cuda_check(cudaGetLastError(), "launch k_crt_tc");
+        cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), smem_crt_, s, pdl, dp_, R, chunk_map(ch),
+                                 npos, nb, out, full),
+                   "launch k_crt_tc");
     } else if (crt_blocked_) {
         const size_t coeffs = (size_t)npos * nb;
         if (poff + coeffs > partial_coeffs_) throw Unsupported("blocked CRT: partial buffers reserved for fewer coefficients");
@@ -734,17 +735,19 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         for (const CrtBlock& b : crt_blocks_) {
             const CrtPartial part{zp, sp, b.mode, b.limb0, b.add_s};
-            k_crt_tc<<<grid, CRT_TC_THREADS, b.smem, s>>>(b.dp, R + (size_t)b.j0 * plan_.N, chunk_map(ch), npos, nb,
-                                                            out, part);
-            cuda_check(cudaGetLastError(), "launch k_crt_tc (block)");
+            cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), b.smem, s, pdl, b.dp,
+                                     R + (size_t)b.j0 * plan_.N, chunk_map(ch), npos, nb, out, part),
+                       "launch k_crt_tc (block)");
+            pdl = true;  // each later launch follows the previous block's
         }
         const size_t fsmem = (size_t)TC_M * crt_zstride(plan_.L) * 4;
-        k_crt_finish<<<(unsigned)((coeffs + TC_M - 1) / TC_M), TC_M, fsmem, s>>>(dp_, zp, sp, (uint32_t)coeffs, out);
-        cuda_check(cudaGetLastError(), "launch k_crt_finish");
+        cuda_check(launch_kernel(k_crt_finish, dim3((unsigned)((coeffs + TC_M - 1) / TC_M)), dim3(TC_M), fsmem, s,
+                                 true, dp_, zp, sp, (uint32_t)coeffs, out),
+                   "launch k_crt_finish");
     } else {
         dim3 grid((npos + CRT_TM - 1) / CRT_TM, 1, nb);
-        k_crt_plain<<<grid, 128, smem_crt_, s>>>(dp_, R, chunk_map(ch), npos, out);
-        cuda_check(cudaGetLastError(), "launch k_crt_plain");
+        cuda_check(launch_kernel(k_crt_plain, grid, dim3(128), smem_crt_, s, pdl, dp_, R, chunk_map(ch), npos, out),
+                   "launch k_crt_plain");
     }
 }
 
@@ -762,14 +765,15 @@ void Engine::run_device(const uint32_t* a, const uint32_t* b, uint32_t* c, uint3
         const uint32_t nb = std::min(g, count - i);
         const uint32_t* ai = a + (size_t)i * cw;
         const uint32_t* bi = b + (size_t)i * cw;
-        launch_dec(ai, all, nb, d_ra_, s, true);
-        launch_cols(false, d_ra_, all, nb, s);
-        launch_rows(false, d_ra_, nullptr, nb, s);
-        launch_dec(bi, all, nb, d_rb_, s);
-        launch_cols(false, d_rb_, all, nb, s);
-        launch_rows(true, d_rb_, d_ra_, nb, s);
-        launch_cols(true, d_rb_, all, nb, s);
-        launch_crt(d_rb_, all, nb, c + (size_t)i * cw, s);
+        // every launch but the call's first follows a kernel of this sequence
+        launch_dec(ai, all, nb, d_ra_, s, true, i > 0);
+        launch_cols(false, d_ra_, all, nb, s, true);
+        launch_rows(false, d_ra_, nullptr, nb, s, nullptr, true);
+        launch_dec(bi, all, nb, d_rb_, s, false, true);
+        launch_cols(false, d_rb_, all, nb, s, true);
+        launch_rows(true, d_rb_, d_ra_, nb, s, nullptr, true);
+        launch_cols(true, d_rb_, all, nb, s, true);
+        launch_crt(d_rb_, all, nb, c + (size_t)i * cw, s, 0, true);
     }
     cuda_check(cudaGetLastError(), "kernel launch");
 }
@@ -832,13 +836,13 @@ void Engine::run_group(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32
     if (nb == 0) return;
     const Chunk all{0, plan_.ncols};
     launch_dec(a, all, nb, ra, s, true);
-    launch_cols(false, ra, all, nb, s);
-    launch_rows(false, ra, nullptr, nb, s);
-    launch_dec(b, all, nb, rb, s);
-    launch_cols(false, rb, all, nb, s);
-    launch_rows(true, rb, ra, nb, s);
-    launch_cols(true, rb, all, nb, s);
-    launch_crt(rb, all, nb, c, s);
+    launch_cols(false, ra, all, nb, s, true);
+    launch_rows(false, ra, nullptr, nb, s, nullptr, true);
+    launch_dec(b, all, nb, rb, s, false, true);
+    launch_cols(false, rb, all, nb, s, true);
+    launch_rows(true, rb, ra, nb, s, nullptr, true);
+    launch_cols(true, rb, all, nb, s, true);
+    launch_crt(rb, all, nb, c, s, 0, true);
     cuda_check(cudaGetLastError(), "kernel launch");
 }
 
@@ -937,7 +941,13 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         const int P = items[i].first;
         const Chunk ch = items[i].second;
         const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
-        cudaStream_t sc = s_comp_[i % 3];
+        // the last input chunk runs on stream 0, after a's row pass and b's other chunks, so
+        // that its kernels, the fused row pass and the first output chunk's follow each other
+        // in one stream (each launch overlapping the previous kernel's tail)
+        const bool last = i + 1 == nin;
+        cudaStream_t sc = last ? s_comp_[0] : s_comp_[i % 3];
+        if (last)
+            for (int k = na; k < i; ++k) cuda_check(cudaStreamWaitEvent(sc, ev_done_in_[k], 0), "wait");
         if (direct_in[P])
             cuda_check(cudaMemcpy2DAsync(d_in_[P] + off, (size_t)ch.cw * L * 4, src[P] + (size_t)ch.col0 * L, pitch,
                                          (size_t)ch.cw * L * 4, nrows, cudaMemcpyHostToDevice, s_h2d_),
@@ -949,13 +959,15 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         mark("h2d" + std::to_string(i), s_h2d_);
         cuda_check(cudaStreamWaitEvent(sc, ev_in_[i], 0), "wait");
         launch_dec(d_in_[P] + off, ch, 1, dR[P], sc, P == 0);
-        launch_cols(false, dR[P], ch, 1, sc);
-        cuda_check(cudaEventRecord(ev_done_in_[i], sc), "record");
-        mark("in" + std::to_string(i), sc);
+        mark("dec" + std::to_string(i), sc);
+        launch_cols(false, dR[P], ch, 1, sc, true);
+        if (!last) {
+            cuda_check(cudaEventRecord(ev_done_in_[i], sc), "record");
+            mark("in" + std::to_string(i), sc);
+        }
         if (i == na - 1) {  // a complete: its row pass overlaps b's transfer
             for (int k = 0; k < na; ++k) cuda_check(cudaStreamWaitEvent(s_comp_[0], ev_done_in_[k], 0), "wait");
             launch_rows(false, d_ra_, nullptr, 1, s_comp_[0]);
-            cuda_check(cudaEventRecord(ev_row_a_, s_comp_[0]), "record");
             mark("rowA", s_comp_[0]);
         }
         if (i + 1 < nin) {
@@ -963,11 +975,10 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
             if (profile_) staged_us.push_back(us(clk::now()));
         }
     }
+    // stream 0 has run a's row pass and b's last chunk after the others
     cudaStream_t s0 = s_comp_[0];
-    cuda_check(cudaStreamWaitEvent(s0, ev_row_a_, 0), "wait");
-    for (int k = na; k < nin; ++k) cuda_check(cudaStreamWaitEvent(s0, ev_done_in_[k], 0), "wait");
-    launch_rows(true, d_rb_, d_ra_, 1, s0);
-    cuda_check(cudaEventRecord(ev_fused_, s0), "record");
+    launch_rows(true, d_rb_, d_ra_, 1, s0, nullptr, true);
+    if (kind == 0) cuda_check(cudaEventRecord(ev_fused_, s0), "record");
     mark("fused", s0);
     for (size_t oc = 0; oc < cout.size(); ++oc) {
         const Chunk ch = cout[oc];
@@ -978,9 +989,10 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         const int si = kind == 1 ? 0 : (int)(oc % 3);
         cudaStream_t sc = s_comp_[si];
         if (si != 0) cuda_check(cudaStreamWaitEvent(sc, ev_fused_, 0), "wait");
-        launch_cols(true, d_rb_, ch, 1, sc);
+        launch_cols(true, d_rb_, ch, 1, sc, si == 0);
+        mark("ci" + std::to_string(oc), sc);
         // output chunks run on three streams: each gets its own region of the partial buffers
-        launch_crt(d_rb_, ch, 1, d_out_ + off, sc, (size_t)ch.col0 * nrows);
+        launch_crt(d_rb_, ch, 1, d_out_ + off, sc, (size_t)ch.col0 * nrows, true);
         cuda_check(cudaEventRecord(ev_crt_[oc], sc), "record");
         mark("crt" + std::to_string(oc), sc);
         cuda_check(cudaStreamWaitEvent(s_d2h_, ev_crt_[oc], 0), "wait");

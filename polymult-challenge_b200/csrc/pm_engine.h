@@ -130,13 +130,17 @@ class Engine {
 
     // launch helpers (also used by the tests' stage-by-stage checks)
     // ra: src is the operand whose transform the fused row pass reads (RA); see pm_engine.cu
-    void launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s, bool ra = false) const;
-    void launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s) const;
+    // pdl: the previous operation in stream s is a kernel; the launch may overlap its tail
+    // (programmatic dependent launch, see launch_kernel)
+    void launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R, cudaStream_t s, bool ra = false,
+                    bool pdl = false) const;
+    void launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s, bool pdl = false) const;
     void launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s,
-                     const uint32_t* ra_sel = nullptr) const;
+                     const uint32_t* ra_sel = nullptr, bool pdl = false) const;
     // `poff`: first coefficient of this launch's region of the blocked CRT's partial buffers --
     // launches that may run concurrently (other streams) must use disjoint regions
-    void launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff = 0) const;
+    void launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff = 0,
+                    bool pdl = false) const;
 
   private:
     struct DecBlock {
@@ -203,7 +207,7 @@ class Engine {
     bool profile_ = false;          // POLYMULT_PROFILE: per-call host and device timeline on stderr
     bool nt_gather_ = true;         // POLYMULT_GATHER_STORES=cached: ordinary stores when staging inputs
     std::vector<cudaEvent_t> trace_ev_;  // timing events of that timeline
-    cudaEvent_t ev_row_a_ = nullptr, ev_fused_ = nullptr;
+    cudaEvent_t ev_fused_ = nullptr;
     std::unique_ptr<HostPool> pool_;
 };
 

@@ -13,14 +13,34 @@ namespace pm {
 
 [[noreturn]] void throw_cuda(cudaError_t e, const char* what);  // throws pm::CudaError
 
+// Launches kernel f.  pdl: with programmatic stream serialization, for a kernel whose previous
+// operation in the stream is a kernel: its prologue (up to pdl_wait()) may then run while that
+// kernel finishes.  Every kernel of the multiply calls pdl_wait() before it reads data another
+// kernel wrote or writes global memory, so the flag changes timing only.
+template <class... KArgs, class... Args>
+inline cudaError_t launch_kernel(void (*f)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl,
+                                 Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, f, static_cast<KArgs>(args)...);
+}
+
 // ---- NTT (k_ntt.cu).  The kernels are templates, so they are launched only from k_ntt.cu
 // (a template kernel launched from another translation unit would bind to a host stub that
 // no module registered); these host wrappers are the interface.
 void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
-                     int ltc);
+                     int ltc, bool pdl = false);
 // fused: batch z of R pairs with transform ra_sel[z] of RA (ra_sel == nullptr: transform z)
 void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
-                     const uint32_t* ra_sel = nullptr);
+                     const uint32_t* ra_sel = nullptr, bool pdl = false);
 // rows of 2^w2 words per row-pass CTA (grid.x = ceil(nrows / this))
 int ntt_rows_per_cta(int w2);
 // line lengths 2^w1 (columns) and 2^w2 (rows) select the compile-time specialisations

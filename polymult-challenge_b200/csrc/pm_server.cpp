@@ -133,11 +133,12 @@ void Server::launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint
     }
     cuda_check(cudaMemcpyAsync(s.sel_d, s.sel_h, nb * 4, cudaMemcpyHostToDevice, s.stream), "selector H2D");
     const Chunk all{0, P.ncols};
+    // after the copies the launches follow one another (each may overlap the previous one's tail)
     eng_->launch_dec(s.in, all, nb, s.res, s.stream);
-    eng_->launch_cols(false, s.res, all, nb, s.stream);
-    eng_->launch_rows(true, s.res, resident_, nb, s.stream, s.sel_d);
-    eng_->launch_cols(true, s.res, all, nb, s.stream);
-    eng_->launch_crt(s.res, all, nb, s.out, s.stream, (size_t)(&s - slots_.data()) * cap_ * P.N);
+    eng_->launch_cols(false, s.res, all, nb, s.stream, true);
+    eng_->launch_rows(true, s.res, resident_, nb, s.stream, s.sel_d, true);
+    eng_->launch_cols(true, s.res, all, nb, s.stream, true);
+    eng_->launch_crt(s.res, all, nb, s.out, s.stream, (size_t)(&s - slots_.data()) * cap_ * P.N, true);
     for (uint32_t i = 0; i < nb; ++i)
         cuda_check(cudaMemcpyAsync(c[s.reqs[i]], s.out + i * cw, cw * 4, cudaMemcpyDeviceToHost, s.stream),
                    "result D2H");
