@@ -465,7 +465,7 @@ void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind) {
     mk(ev_done_in_, nin, cudaEventDisableTiming);
     mk(ev_crt_, nco, cudaEventDisableTiming);
     mk(ev_out_, nco, cudaEventDisableTiming);
-    if (profile_) mk(trace_ev_, 8 + 3 * nin + 3 * nco, cudaEventDefault);
+    if (profile_) mk(trace_ev_, 8 + 2 * nin + 2 * nco, cudaEventDefault);
 }
 
 double Engine::tune_host_pipeline(int reps, int kind) {
@@ -959,7 +959,6 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         mark("h2d" + std::to_string(i), s_h2d_);
         cuda_check(cudaStreamWaitEvent(sc, ev_in_[i], 0), "wait");
         launch_dec(d_in_[P] + off, ch, 1, dR[P], sc, P == 0);
-        mark("dec" + std::to_string(i), sc);
         launch_cols(false, dR[P], ch, 1, sc, true);
         if (!last) {
             cuda_check(cudaEventRecord(ev_done_in_[i], sc), "record");
@@ -990,7 +989,6 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         cudaStream_t sc = s_comp_[si];
         if (si != 0) cuda_check(cudaStreamWaitEvent(sc, ev_fused_, 0), "wait");
         launch_cols(true, d_rb_, ch, 1, sc, si == 0);
-        mark("ci" + std::to_string(oc), sc);
         // output chunks run on three streams: each gets its own region of the partial buffers
         launch_crt(d_rb_, ch, 1, d_out_ + off, sc, (size_t)ch.col0 * nrows, true);
         cuda_check(cudaEventRecord(ev_crt_[oc], sc), "record");
