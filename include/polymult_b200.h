@@ -79,10 +79,11 @@ int pm_run_device(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uin
 enum pm_stage {
     PM_STAGE_DEC_A = 0,    /* RNS decomposition of a */
     PM_STAGE_COLS_A = 1,   /* forward column pass of a */
-    PM_STAGE_ROWS_A = 2,   /* forward row pass of a */
+    PM_STAGE_ROWS_A = 2,   /* forward row pass of a: 0 in device-resident groups, whose row pass
+                              (PM_STAGE_FUSED) transforms both operands' rows */
     PM_STAGE_DEC_B = 3,    /* RNS decomposition of b */
     PM_STAGE_COLS_B = 4,   /* forward column pass of b */
-    PM_STAGE_FUSED = 5,    /* fused row pass: forward b, pointwise with a, inverse */
+    PM_STAGE_FUSED = 5,    /* fused row pass: forward rows of b and a, pointwise, inverse */
     PM_STAGE_COLS_INV = 6, /* inverse column pass */
     PM_STAGE_CRT = 7       /* CRT straight to mod q */
 };

@@ -60,6 +60,27 @@ __device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const StwF& st
     }
 }
 
+// The forward network on two operands' lines that share their twiddles (the same prime and
+// row): each twiddle is read once for both butterflies.
+template <int RB, int T0, class StwF>
+__device__ __forceinline__ void radix_fwd2(uint32_t (&v)[1 << RB], uint32_t (&u)[1 << RB], const StwF& stw,
+                                           uint32_t p) {
+#pragma unroll
+    for (int t = T0; t < RB; ++t) {
+        const int h = (1 << RB) >> (t + 1);
+        const auto w = stw(t);
+#pragma unroll
+        for (int m = 0; m < (1 << t); ++m) {
+            const Tw2 wm = w[m];
+#pragma unroll
+            for (int i = 0; i < h; ++i) {
+                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                bfly_ct_sh(u[m * 2 * h + i], u[m * 2 * h + i + h], wm, p);
+            }
+        }
+    }
+}
+
 // Inverse (GS) network, local stages RB-1 down to T0, mirrored twiddles from stw(t).
 template <int RB, int T0, class StwF>
 __device__ __forceinline__ void radix_inv(uint32_t (&v)[1 << RB], const StwF& stw, uint32_t p) {
@@ -246,6 +267,33 @@ __device__ __forceinline__ void row_forward(uint32_t (&v)[RowCfg<NB>::E], uint32
     }
 }
 
+// row_forward on two operands' rows of the same prime and row index (b in v, a in u), each in
+// its own shared-memory region for the exchanges.
+template <int NB, int K>
+__device__ __forceinline__ void row_forward2(uint32_t (&v)[RowCfg<NB>::E], uint32_t (&u)[RowCfg<NB>::E],
+                                             uint32_t* region, uint32_t* region_u, int rho, int r, const uint2* twj,
+                                             int w1, uint32_t hi, uint32_t p) {
+    using C = RowCfg<NB>;
+    if constexpr (K < C::NPH) {
+        constexpr int b0 = C::b0(K);
+        const uint32_t hip = (uint32_t)(r >> b0);
+        auto stw = [&](int t) {
+            const int ls = C::ls(K, t);
+            return RunTw<false>{twj + (1u << (w1 + ls)) + (hi << ls) + (hip << t), 1 << t};
+        };
+        radix_fwd2<C::RB, C::t0(K)>(v, u, stw, p);
+        if constexpr (K + 1 < C::NPH) {
+            row_xchg<NB, K, true>(v, region, rho, r);
+            row_xchg<NB, K, true>(u, region_u, rho, r);
+            region_sync<NB>();
+            row_xchg<NB, K + 1, false>(v, region, rho, r);
+            row_xchg<NB, K + 1, false>(u, region_u, rho, r);
+            region_sync<NB>();
+            row_forward2<NB, K + 1>(v, u, region, region_u, rho, r, twj, w1, hi, p);
+        }
+    }
+}
+
 // Inverse phases K down to 0 (registers in the layout of phase K on entry, phase 0 on exit).
 // The inverse twiddle of (ls, hi, gi) is the forward entry of the mirrored row nrows-1-hi at
 // 2^ls - 1 - gi.
@@ -276,19 +324,27 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
 }  // namespace
 
 // Row pass over ROWS_PER_CTA consecutive rows of one prime and batch entry, 128 threads.
-//   FUSED = false: forward row stages (operand a).
-//   FUSED = true : forward row stages of b, pointwise product with the finished transform of
-//                  a (RA), inverse row stages.  The Montgomery pointwise product leaves a
-//                  factor 2^-32 that the CRT constant crt_c compensates.  Batch z pairs with
-//                  transform ra_sel[z] of RA when ra_sel is given (a server's resident
-//                  operands), else with transform z.
-// Blocks per SM: the most at which no variant spills (64 registers at 8, 80 at 6, 96 at 5,
-// 128 at 4); the fused kernel holds the other operand's row and more twiddle runs.
-template <int NB, bool FUSED>
-__global__ void __launch_bounds__(128, NB >= 9 ? (FUSED ? 4 : 5) : (FUSED ? 6 : 8)) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R, const uint32_t* __restrict__ RA,
-                                                  const uint32_t* __restrict__ ra_sel) {
+//   ROWS_FWD  : forward row stages (operand a).
+//   ROWS_FUSED: forward row stages of b, pointwise product with the finished transform of a
+//               (RA), inverse row stages.  Batch z pairs with transform ra_sel[z] of RA when
+//               ra_sel is given (a server's resident operands), else with transform z.
+//   ROWS_BOTH : forward row stages of b and of a (RA, after its column pass) side by side,
+//               each twiddle read once for both, then the pointwise product and the inverse
+//               stages of b; RA is read and not written.
+// The Montgomery pointwise product leaves a factor 2^-32 that the CRT constant crt_c
+// compensates.  Blocks per SM: the most at which no variant spills (64 registers at 8, 80 at
+// 6, 96 at 5, 128 at 4); the fused kernels hold the other operand's row and more twiddle runs.
+enum : int { ROWS_FWD = 0, ROWS_FUSED = 1, ROWS_BOTH = 2 };
+__host__ __device__ constexpr int rows_min_blocks(int nb, int mode) {
+    return nb >= 9 ? (mode == ROWS_FWD ? 5 : 4) : (mode == ROWS_FWD ? 8 : mode == ROWS_FUSED ? 6 : 5);
+}
+template <int NB, int MODE>
+__global__ void __launch_bounds__(128, rows_min_blocks(NB, MODE)) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R,
+                                                                           const uint32_t* __restrict__ RA,
+                                                                           const uint32_t* __restrict__ ra_sel) {
     using C = RowCfg<NB>;
-    __shared__ __align__(16) uint32_t sh[C::NPH > 1 ? 128 * C::E : 4];
+    constexpr int REGION_WORDS = C::NPH > 1 ? 128 * C::E : 4;
+    __shared__ __align__(16) uint32_t sh[MODE == ROWS_BOTH ? 2 * REGION_WORDS : REGION_WORDS];
     const int tid = threadIdx.x;
     const int li = tid % C::GRP;                 // thread within the shared-memory region
     const int rho = li / C::LPR, r = li % C::LPR;
@@ -312,8 +368,16 @@ __global__ void __launch_bounds__(128, NB >= 9 ? (FUSED ? 4 : 5) : (FUSED ? 6 : 
     pdl_trigger();
     pdl_wait();
     row_global<NB, 0, true>(v, row, r, active);
-    row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p);
-    if constexpr (FUSED) {
+    if constexpr (MODE == ROWS_BOTH) {
+        uint32_t a[C::E];
+        row_global<NB, 0, true>(a, const_cast<uint32_t*>(RA + off), r, active);
+        row_forward2<NB, 0>(v, a, region, region + REGION_WORDS, rho, r, twj, P.w1, hic, p);
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) v[e] = mont_mul(red_once(red_once(a[e], 2 * p), p), v[e], p, pinv);
+        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p);
+        row_global<NB, 0, false>(v, row, r, active);
+    } else if constexpr (MODE == ROWS_FUSED) {
+        row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p);
         uint32_t a[C::E];
         const size_t za = ra_sel ? (size_t)__ldg(ra_sel + zb) : (size_t)zb;
         const size_t offa = (za * P.K + j) * P.N + (size_t)hic * (1u << NB);
@@ -323,6 +387,7 @@ __global__ void __launch_bounds__(128, NB >= 9 ? (FUSED ? 4 : 5) : (FUSED ? 6 : 
         row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p);
         row_global<NB, 0, false>(v, row, r, active);
     } else {
+        row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p);
         row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), false>(v, row, r, active);
     }
 }
@@ -432,11 +497,16 @@ void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevP
 }
 
 template <int NB>
-void launch_rows_nb(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
+void launch_rows_nb(int mode, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
                     const uint32_t* ra_sel, bool pdl) {
-    const cudaError_t e = launch_kernel(fused ? k_ntt_rows<NB, true> : k_ntt_rows<NB, false>, grid, dim3(128), 0, s,
-                                        pdl, P, R, RA, ra_sel);
-    if (e != cudaSuccess) throw_cuda(e, fused ? "launch k_ntt_rows<fused>" : "launch k_ntt_rows<forward>");
+    const cudaError_t e = launch_kernel(mode == ROWS_BOTH    ? k_ntt_rows<NB, ROWS_BOTH>
+                                        : mode == ROWS_FUSED ? k_ntt_rows<NB, ROWS_FUSED>
+                                                             : k_ntt_rows<NB, ROWS_FWD>,
+                                        grid, dim3(128), 0, s, pdl, P, R, RA, ra_sel);
+    if (e != cudaSuccess)
+        throw_cuda(e, mode == ROWS_BOTH    ? "launch k_ntt_rows<both operands>"
+                      : mode == ROWS_FUSED ? "launch k_ntt_rows<fused>"
+                                           : "launch k_ntt_rows<forward>");
 }
 
 // Applies F<NB>::run(...) for the line length 2^nb, nb in [0, 10].
@@ -492,7 +562,8 @@ struct ColProbeF {
 template <int NB>
 struct RowProbeF {
     static void run() {
-        const void* fns[2] = {(const void*)k_ntt_rows<NB, false>, (const void*)k_ntt_rows<NB, true>};
+        const void* fns[3] = {(const void*)k_ntt_rows<NB, ROWS_FWD>, (const void*)k_ntt_rows<NB, ROWS_FUSED>,
+                              (const void*)k_ntt_rows<NB, ROWS_BOTH>};
         for (const void* f : fns) {
             cudaFuncAttributes fa{};
             const cudaError_t e = cudaFuncGetAttributes(&fa, f);
@@ -512,9 +583,9 @@ void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const Dev
     dispatch_nb<ColsF>(P.w1, inv, grid, smem, s, P, R, col0, ltc, pdl);
 }
 
-void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
+void launch_ntt_rows(int mode, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
                      const uint32_t* ra_sel, bool pdl) {
-    dispatch_nb<RowsF>(P.w2, fused, grid, s, P, R, RA, ra_sel, pdl);
+    dispatch_nb<RowsF>(P.w2, mode, grid, s, P, R, RA, ra_sel, pdl);
 }
 
 int ntt_rows_per_cta(int w2) {

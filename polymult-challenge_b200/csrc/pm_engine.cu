@@ -661,7 +661,8 @@ void Engine::reserve_crt_partials(size_t coeffs) {
 int Engine::kernel_launches_per_group() const {
     const int dec = dec_tc_ ? (int)dec_blocks_.size() : 1;
     const int crt = crt_blocked_ ? (int)crt_blocks_.size() + 1 : 1;
-    return 2 * dec + crt + (plan_.w1 > 0 ? 5 : 3);
+    // column passes of a, b and the inverse, and one row pass for both operands
+    return 2 * dec + crt + (plan_.w1 > 0 ? 4 : 1);
 }
 
 ChunkMap Engine::chunk_map(Chunk ch) const {
@@ -716,6 +717,11 @@ void Engine::launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t n
     launch_ntt_rows(fused, grid, s, dp_, R, RA, ra_sel, pdl);
 }
 
+void Engine::launch_rows_both(uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s, bool pdl) const {
+    dim3 grid((plan_.nrows + rpb_ - 1) / rpb_, plan_.K, nb);
+    launch_ntt_rows(2, grid, s, dp_, R, RA, nullptr, pdl);
+}
+
 void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff,
                         bool pdl) const {
     const uint32_t npos = plan_.nrows * ch.cw;
@@ -768,10 +774,9 @@ void Engine::run_device(const uint32_t* a, const uint32_t* b, uint32_t* c, uint3
         // every launch but the call's first follows a kernel of this sequence
         launch_dec(ai, all, nb, d_ra_, s, true, i > 0);
         launch_cols(false, d_ra_, all, nb, s, true);
-        launch_rows(false, d_ra_, nullptr, nb, s, nullptr, true);
         launch_dec(bi, all, nb, d_rb_, s, false, true);
         launch_cols(false, d_rb_, all, nb, s, true);
-        launch_rows(true, d_rb_, d_ra_, nb, s, nullptr, true);
+        launch_rows_both(d_rb_, d_ra_, nb, s, true);
         launch_cols(true, d_rb_, all, nb, s, true);
         launch_crt(d_rb_, all, nb, c + (size_t)i * cw, s, 0, true);
     }
@@ -791,18 +796,19 @@ void Engine::time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint
     double acc[S] = {0};
     try {
         for (int r = 0; r < reps; ++r) {
+            // the sequence of run_device; stage 2 (a's own row pass) is empty, as the row pass
+            // of stage 5 transforms both operands' rows
             cuda_check(cudaEventRecord(ev[0], s), "record");
             launch_dec(a, all, count, d_ra_, s, true);
             cuda_check(cudaEventRecord(ev[1], s), "record");
             launch_cols(false, d_ra_, all, count, s);
             cuda_check(cudaEventRecord(ev[2], s), "record");
-            launch_rows(false, d_ra_, nullptr, count, s);
             cuda_check(cudaEventRecord(ev[3], s), "record");
             launch_dec(b, all, count, d_rb_, s);
             cuda_check(cudaEventRecord(ev[4], s), "record");
             launch_cols(false, d_rb_, all, count, s);
             cuda_check(cudaEventRecord(ev[5], s), "record");
-            launch_rows(true, d_rb_, d_ra_, count, s);
+            launch_rows_both(d_rb_, d_ra_, count, s);
             cuda_check(cudaEventRecord(ev[6], s), "record");
             launch_cols(true, d_rb_, all, count, s);
             cuda_check(cudaEventRecord(ev[7], s), "record");
@@ -811,6 +817,7 @@ void Engine::time_stages(const uint32_t* a, const uint32_t* b, uint32_t* c, uint
             cuda_check(cudaGetLastError(), "kernel launch");
             cuda_check(cudaEventSynchronize(ev[S]), "sync");
             for (int k = 0; k < S; ++k) {
+                if (k == 2) continue;  // no kernel between ev[2] and ev[3]
                 float ms = 0;
                 cuda_check(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "elapsed");
                 acc[k] += ms;
@@ -837,10 +844,9 @@ void Engine::run_group(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32
     const Chunk all{0, plan_.ncols};
     launch_dec(a, all, nb, ra, s, true);
     launch_cols(false, ra, all, nb, s, true);
-    launch_rows(false, ra, nullptr, nb, s, nullptr, true);
     launch_dec(b, all, nb, rb, s, false, true);
     launch_cols(false, rb, all, nb, s, true);
-    launch_rows(true, rb, ra, nb, s, nullptr, true);
+    launch_rows_both(rb, ra, nb, s, true);
     launch_cols(true, rb, all, nb, s, true);
     launch_crt(rb, all, nb, c, s, 0, true);
     cuda_check(cudaGetLastError(), "kernel launch");

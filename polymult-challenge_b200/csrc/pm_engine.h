@@ -137,6 +137,9 @@ class Engine {
     void launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s, bool pdl = false) const;
     void launch_rows(bool fused, uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s,
                      const uint32_t* ra_sel = nullptr, bool pdl = false) const;
+    // both operands' row passes in one kernel: forward rows of R (b) and RA (a, after its column
+    // pass, read only), pointwise product, inverse rows into R
+    void launch_rows_both(uint32_t* R, const uint32_t* RA, uint32_t nb, cudaStream_t s, bool pdl = false) const;
     // `poff`: first coefficient of this launch's region of the blocked CRT's partial buffers --
     // launches that may run concurrently (other streams) must use disjoint regions
     void launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff = 0,

@@ -38,8 +38,11 @@ inline cudaError_t launch_kernel(void (*f)(KArgs...), dim3 grid, dim3 block, siz
 // no module registered); these host wrappers are the interface.
 void launch_ntt_cols(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
                      int ltc, bool pdl = false);
-// fused: batch z of R pairs with transform ra_sel[z] of RA (ra_sel == nullptr: transform z)
-void launch_ntt_rows(bool fused, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
+// mode 0: forward row stages of R; 1 (fused): forward, pointwise product with RA's finished
+// transform (batch z of R pairs with transform ra_sel[z] of RA; ra_sel == nullptr: transform z),
+// inverse; 2 (both): forward stages of R and of RA (after its column pass) side by side,
+// pointwise, inverse stages into R
+void launch_ntt_rows(int mode, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
                      const uint32_t* ra_sel = nullptr, bool pdl = false);
 // rows of 2^w2 words per row-pass CTA (grid.x = ceil(nrows / this))
 int ntt_rows_per_cta(int w2);
