@@ -42,7 +42,9 @@ METRIC = "mults/s at N=65536 W=1747 (bit-exact): tensor-core+batched vs plain; p
 
 # algorithmic HBM bytes of each kernel for ONE multiply (a launch of B multiplies moves B times this):
 #   decomposition: N*L*4 in + K*N*4 out; column/row passes: K*N*4 in + out;
-#   fused row pass: 2*K*N*4 in + K*N*4 out; CRT: K*N*4 in + N*L*4 out
+#   row pass of both operands (forward rows of a and b, pointwise, inverse rows of b; the
+#   device-resident group's "rows_fused" stage, its "rows_a" stage then empty): 2*K*N*4 in +
+#   K*N*4 out; CRT: K*N*4 in + N*L*4 out
 def stage_bytes(stage, N, L, K):
     rn, cw = K * N * 4, N * L * 4
     return {"dec_a": cw + rn, "dec_b": cw + rn, "cols_a": 2 * rn, "cols_b": 2 * rn, "rows_a": 2 * rn,
