@@ -332,11 +332,13 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
 //               each twiddle read once for both, then the pointwise product and the inverse
 //               stages of b; RA is read and not written.
 // The Montgomery pointwise product leaves a factor 2^-32 that the CRT constant crt_c
-// compensates.  Blocks per SM: the most at which no variant spills (64 registers at 8, 80 at
-// 6, 96 at 5, 128 at 4); the fused kernels hold the other operand's row and more twiddle runs.
+// compensates.  Blocks per SM: the most at which the variants do not spill (64 registers at 8,
+// 80 at 6, 128 at 4); the fused kernels hold the other operand's row and more twiddle runs.
+// The two-operand form at 6 (80 registers) ran its pass in 34.2 us per multiply against 36.1 at
+// 5 (96) and 37.4 at 4 (117) (N=65536, W=1747, launches of 8); at 7 it spills.
 enum : int { ROWS_FWD = 0, ROWS_FUSED = 1, ROWS_BOTH = 2 };
 __host__ __device__ constexpr int rows_min_blocks(int nb, int mode) {
-    return nb >= 9 ? (mode == ROWS_FWD ? 5 : 4) : (mode == ROWS_FWD ? 8 : mode == ROWS_FUSED ? 6 : 5);
+    return nb >= 9 ? (mode == ROWS_FWD ? 5 : 4) : (mode == ROWS_FWD ? 8 : 6);
 }
 template <int NB, int MODE>
 __global__ void __launch_bounds__(128, rows_min_blocks(NB, MODE)) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R,
