@@ -129,6 +129,30 @@ def test_commutative_and_linear():
     assert orc.unpack_limbs(sb) == exp
 
 
+def test_stage_timing_runs_the_device_sequence():
+    """pm_time_stages times the device-resident sequence kernel by kernel: every kernel stage
+    takes time, a's own row pass is empty (the row pass of both operands covers it), and the
+    timed launches leave the exact products in c."""
+    torch = _torch()
+    import polymult
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (32768, 868))
+    q = int(pt["q_hex"], 16)
+    A = [orc.uniform_limbs(32768, 868, q, seed=41 + i) for i in range(2)]
+    B = [orc.uniform_limbs(32768, 868, q, seed=51 + i) for i in range(2)]
+    da = torch.from_numpy(np.stack(A).view(np.int32)).cuda()
+    db = torch.from_numpy(np.stack(B).view(np.int32)).cuda()
+    dc = torch.zeros_like(da)
+    with _multiplier(pt, "tensor") as m:
+        st = m.time_stages(da.data_ptr(), db.data_ptr(), dc.data_ptr(), 2, 3, torch.cuda.current_stream().cuda_stream)
+        m.sync()
+    assert list(st) == list(polymult.STAGES)
+    assert st["rows_a"] == 0.0
+    assert all(v > 0 for k, v in st.items() if k != "rows_a"), st
+    out = dc.cpu().numpy().view(np.uint32)
+    for i in range(2):
+        assert np.array_equal(out[i], c_oracle_mul(32768, 868, q, A[i], B[i])), i
+
+
 def test_fherma_python_mirror():
     import polymult
     pt = next(p for p in POINTS if (p["N"], p["W"]) == (4096, 256))
