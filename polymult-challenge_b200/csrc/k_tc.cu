@@ -120,14 +120,15 @@ __device__ __forceinline__ uint32_t idesc_u8(int n) {
 }
 
 // Issues D[:, col0 : col0 + nn) = A * B[row0 : row0 + nn, :]^T into TMEM column col0.
+// acc: the first MMA adds to the accumulator too (a further block of the K dimension)
 __device__ __forceinline__ void issue_gemm_rows(uint32_t tmem_col, uint32_t a_base, uint32_t b_base, int row0, int nn,
-                                                int kbytes) {
+                                                int kbytes, bool acc = false) {
     const uint32_t sbo = 8u * (uint32_t)kbytes;
     const uint32_t idesc = idesc_u8(nn);
     for (int kk = 0; kk < kbytes / 32; ++kk) {
         const uint64_t ad = sdesc(a_base + 256u * kk, 128u, sbo);
         const uint64_t bd = sdesc(b_base + (uint32_t)(row0 >> 3) * sbo + 256u * kk, 128u, sbo);
-        umma_u8(tmem_col, ad, bd, idesc, kk > 0 ? 1u : 0u);
+        umma_u8(tmem_col, ad, bd, idesc, (kk > 0 || acc) ? 1u : 0u);
     }
 }
 
@@ -476,7 +477,7 @@ __device__ __forceinline__ CrtSmem crt_smem(unsigned char* base, const DevPlan& 
     m.rcp = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(m.z) + crt_z_bytes(P));
     m.spart = m.rcp + P.KP;
     m.bars = reinterpret_cast<uint64_t*>(m.spart + 4 * TC_M);
-    m.slot = reinterpret_cast<uint32_t*>(m.bars + 7);
+    m.slot = reinterpret_cast<uint32_t*>(m.bars + 8);  // bars: B, mma_done 2, acc_empty 2, v_ready 2, ab_free
     m.abort = reinterpret_cast<volatile int*>(m.slot + 1);
     return m;
 }
@@ -485,7 +486,8 @@ __device__ __forceinline__ CrtSmem crt_smem(unsigned char* base, const DevPlan& 
 
 __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const uint32_t* __restrict__ R, ChunkMap C,
                                                               uint32_t npos, uint32_t nbatch,
-                                                              uint32_t* __restrict__ out, CrtPartial part) {
+                                                              uint32_t* __restrict__ out, CrtPartial part,
+                                                              CrtPrimeBlocks pbs) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const CrtSmem S = crt_smem(smem_raw, P);
     // partial modes: the block's integer (and, if add_s, its share of sum y_j / p_j) goes into
@@ -508,8 +510,9 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             mbar_init(acc_empty + k, CRT_EPI_THREADS);
             mbar_init(v_ready + k, 1);
         }
+        mbar_init(S.bars + 7, 1);  // ab_free: a prime block's MMAs have read A and B
         *S.abort = 0;
-        bulk_g2s_all(S.b, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
+        if (pbs.n == 0) bulk_g2s_all(S.b, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);  // else per block
     }
     for (int j = threadIdx.x; j < KP; j += blockDim.x) S.rcp[j] = P.rcp[j];
     if (warp == 0) tmem_alloc(S.slot, 2 * AS);
@@ -521,8 +524,12 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     tc_fence_after();
     pdl_trigger();  // after this block's TMEM allocation
     const uint32_t tmem = *S.slot;
-    uint32_t issued = 0;  // tiles whose MMAs thread 0 issued
-    bool b_seen = false;  // thread 0 has seen the B image land
+    uint32_t issued = 0;         // tiles whose MMAs thread 0 issued
+    bool b_seen = pbs.n != 0;    // thread 0 has seen the (one) B image land
+    uint64_t* ab_free = S.bars + 7;
+    uint32_t ab_commits = 0;     // thread 0: prime-block MMA groups committed to ab_free
+    bool b_pend = false;         // thread 0: a per-block B copy nobody has waited for (parity b_par)
+    uint32_t b_par = 0;
 
     if (threadIdx.x < CRT_PROD_THREADS) {
         // ---------------- producers ----------------
@@ -535,13 +542,14 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         // the same residue mod q, v' <= 2K - 1 <= 255 still fits A's v byte, and the fractional
         // part of the sum, which the exactness check reads, is unchanged.  The padding primes
         // K..KP-1 meet zero B columns (but for A's v column, written after them) and 1/p = 0.
+        // With prime blocks (pbs.n > 0) a tile runs the blocks in turn: each block's residues into
+        // A and (thread 0) its B image into S.b once the previous block's MMAs have read them
+        // (ab_free), its MMAs accumulating into the tile's accumulator; the sums of y'_j / p_j run
+        // over all blocks.
         const int m = threadIdx.x & (TC_M - 1), h = threadIdx.x >> 7;
-        const int G = KP / 4;
-        const int gh = (G + 1) / 2;
-        const int g0 = h ? gh : 0, ng = (h ? G : gh) - g0;
         const size_t N = P.N;
-        unsigned char* arow = S.a + (size_t)(m >> 3) * sbo + (m & 7) * 16;
-        uint32_t i = 0;
+        const int npb = pbs.n > 0 ? pbs.n : 1;
+        uint32_t i = 0, seq = 0;  // seq: prime-block MMA groups so far (npb per tile)
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(1, CRT_PROD_THREADS, *S.abort != 0)) break;
             const int b = (int)(i & 1);
@@ -550,61 +558,97 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             // positions past the end of the batch repeat the tile's first one: their A rows and
             // partial sums only feed accumulator rows the epilogue does not store
             const uint32_t pm = (uint32_t)m < npos - pos0 ? pos0 + m : pos0;
-            const uint32_t* rp = R + (size_t)bt * P.Kr * N + chunk_pos_to_n(P, C, pm) + (size_t)(4 * g0) * N;
-            // the previous tile's MMA must have read the A tile before it is overwritten
-            if (i > 0) wait_or_abort(mma_done + ((i - 1) & 1), ((i - 1) >> 1) & 1, S.abort);
-            // every residue of this thread's primes straight into its A row with 4-byte async
-            // copies: no register staging, the whole tile in flight at once (register batches
-            // held ~24 KB per SM in flight and left the loads latency-bound); prime slots past K
-            // re-read prime K-1
-#pragma unroll 2
-            for (int gg = 0; gg < ng; ++gg) {
-                const int g = g0 + gg;
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    cp_async4(arow + (size_t)g * 128 + 4 * k, rp + (size_t)(min(4 * g + k, K - 1) - 4 * g0) * N);
-            }
-            cp_async_wait_all();
-            // sum y'_j / p_j over this thread's primes, read back from its A row
+            const uint32_t* rtile = R + (size_t)bt * P.Kr * N + chunk_pos_to_n(P, C, pm);
             float s4[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int pb = 0; pb < npb; ++pb, ++seq) {
+                const int j0b = pbs.n ? pbs.j0[pb] : 0, Kb = pbs.n ? pbs.k[pb] : K;
+                const int KPb = pbs.n ? pbs.kp[pb] : KP, kbb = pbs.n ? pbs.kb[pb] : kb;
+                const int G = KPb / 4;
+                const int gh = (G + 1) / 2;
+                const int g0 = h ? gh : 0, ng = (h ? G : gh) - g0;
+                unsigned char* arow = S.a + (size_t)(m >> 3) * (8 * kbb) + (m & 7) * 16;
+                const uint32_t* rp = rtile + (size_t)(j0b + 4 * g0) * N;
+                // the previous MMA group must have read A (and B) before they are overwritten
+                if (pbs.n) {
+                    if (seq > 0) wait_or_abort(ab_free, (seq - 1) & 1, S.abort);
+                    if (threadIdx.x == 0) {
+                        bulk_g2s_all(S.b, pbs.b[pb], (uint32_t)((size_t)nrows_b * kbb), bar_b);
+                        b_pend = true;
+                        b_par = seq & 1;
+                    }
+                } else if (i > 0) {
+                    wait_or_abort(mma_done + ((i - 1) & 1), ((i - 1) >> 1) & 1, S.abort);
+                }
+                // every residue of this thread's primes straight into its A row with 4-byte async
+                // copies: no register staging, the whole tile in flight at once (register batches
+                // held ~24 KB per SM in flight and left the loads latency-bound); prime slots past
+                // the block's last prime re-read it
+#pragma unroll 2
+                for (int gg = 0; gg < ng; ++gg) {
+                    const int g = g0 + gg;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        cp_async4(arow + (size_t)g * 128 + 4 * k, rp + (size_t)(min(4 * g + k, Kb - 1) - 4 * g0) * N);
+                }
+                cp_async_wait_all();
+                // sum y'_j / p_j over this thread's primes, read back from its A row
 #pragma unroll 4
-            for (int gg = 0; gg < ng; ++gg) {
-                const int g = g0 + gg;
-                const uint4 x = *reinterpret_cast<const uint4*>(arow + (size_t)g * 128);
-                const float4 r = *reinterpret_cast<const float4*>(S.rcp + 4 * g);
-                s4[0] = fmaf((float)x.x, r.x, s4[0]);
-                s4[1] = fmaf((float)x.y, r.y, s4[1]);
-                s4[2] = fmaf((float)x.z, r.z, s4[2]);
-                s4[3] = fmaf((float)x.w, r.w, s4[3]);
-            }
-            // the epilogue of tile i - 2 must have read partial sums [b] (it arrives on
-            // acc_empty[b] after that)
-            if (i > 1) wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
-            S.spart[(b * 2 + h) * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
-            if (part.mode == CRT_FULL) {
-                // v = round(sum y_j / p_j) (|x| < M/8 keeps the sum within 1/8 of an integer;
-                // further than 1/4 is a failed check) into A's v column: the MMA adds v T_1
+                for (int gg = 0; gg < ng; ++gg) {
+                    const int g = g0 + gg;
+                    const uint4 x = *reinterpret_cast<const uint4*>(arow + (size_t)g * 128);
+                    const float4 r = *reinterpret_cast<const float4*>(S.rcp + j0b + 4 * g);
+                    s4[0] = fmaf((float)x.x, r.x, s4[0]);
+                    s4[1] = fmaf((float)x.y, r.y, s4[1]);
+                    s4[2] = fmaf((float)x.z, r.z, s4[2]);
+                    s4[3] = fmaf((float)x.w, r.w, s4[3]);
+                }
+                const bool last = pb + 1 == npb;
+                if (last) {
+                    // the epilogue of tile i - 2 must have read partial sums [b] (it arrives on
+                    // acc_empty[b] after that)
+                    if (i > 1) wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
+                    S.spart[(b * 2 + h) * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+                    if (part.mode == CRT_FULL) {
+                        // v = round(sum y_j / p_j) (|x| < M/8 keeps the sum within 1/8 of an integer;
+                        // further than 1/4 is a failed check) into A's v column: the MMA adds v T_1
+                        named_sync(1, CRT_PROD_THREADS);
+                        if (h == 0) {
+                            const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
+                            const float vf = rintf(sum);
+                            if ((uint32_t)m < npos - pos0 && fabsf(sum - vf) > 0.25f)
+                                flag_error(P.status, DEV_ERR_CRT_BOUND);
+                            arow[(size_t)(P.crt_kv >> 4) * 128 + (P.crt_kv & 15)] =
+                                (unsigned char)min(max((int)vf, 0), 2 * K - 1);
+                        }
+                    }
+                }
+                fence_smem_to_async();
                 named_sync(1, CRT_PROD_THREADS);
-                if (h == 0) {
-                    const float sum = S.spart[(b * 2) * TC_M + m] + S.spart[(b * 2 + 1) * TC_M + m];
-                    const float vf = rintf(sum);
-                    if ((uint32_t)m < npos - pos0 && fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
-                    arow[(size_t)(P.crt_kv >> 4) * 128 + (P.crt_kv & 15)] = (unsigned char)min(max((int)vf, 0), 2 * K - 1);
+                if (threadIdx.x == 0) {
+                    bool ok = *S.abort == 0;
+                    if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, S.abort);
+                    if (ok && pbs.n) {
+                        ok = wait_or_abort(bar_b, seq & 1, S.abort);
+                        if (ok) b_pend = false;
+                        // the block's first MMA starts the accumulator afresh: tile i - 2's
+                        // epilogue must have read it
+                        if (ok && pb == 0 && i > 1) ok = wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
+                    }
+                    if (ok) {
+                        tc_fence_after();
+                        const uint32_t acc = tmem + (uint32_t)b * AS;
+                        issue_gemm_rows(acc, smem_addr(S.a), smem_addr(S.b), 0, nrows_b, kbb, pb > 0);
+                        if (pbs.n) {
+                            umma_commit(ab_free);
+                            ++ab_commits;
+                        }
+                        if (last) {
+                            umma_commit(mma_done + b);
+                            ++issued;
+                        }
+                    }
+                    if (last) mbar_arrive(v_ready + b);  // releases this tile's partial sums
                 }
-            }
-            fence_smem_to_async();
-            named_sync(1, CRT_PROD_THREADS);
-            if (threadIdx.x == 0) {
-                bool ok = *S.abort == 0;
-                if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, S.abort);
-                if (ok) {
-                    tc_fence_after();
-                    const uint32_t acc = tmem + (uint32_t)b * AS;
-                    issue_gemm_rows(acc, smem_addr(S.a), smem_addr(S.b), 0, nrows_b, kb);
-                    umma_commit(mma_done + b);
-                    ++issued;
-                }
-                mbar_arrive(v_ready + b);  // releases this tile's partial sums
             }
         }
     } else {
@@ -765,7 +809,10 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         // copies and MMAs still in flight must land before this CTA's memory goes away
         if (!b_seen) mbar_wait_bounded(bar_b, 0);
         if (issued) mbar_wait_bounded(mma_done + ((issued - 1) & 1), ((issued - 1) >> 1) & 1);
+        if (b_pend) mbar_wait_bounded(bar_b, b_par);
     }
+    // the last prime block's ab_free arrival (its MMAs are complete: the epilogue waited for them)
+    if (threadIdx.x == 0 && ab_commits) mbar_wait_bounded(ab_free, (ab_commits - 1) & 1);
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, 2 * AS);
 }
@@ -777,7 +824,7 @@ size_t rns_tc_smem(const DevPlan& P) {
 
 size_t crt_tc_smem(const DevPlan& P, bool partial) {
     return (size_t)P.crt_nrows * P.crt_kbytes + (size_t)TC_M * P.crt_kbytes + crt_z_bytes(P) + (size_t)P.KP * 4 +
-           4 * TC_M * 4 + 7 * 8 + 32 + (partial ? crt_z_bytes(P) : 0);
+           4 * TC_M * 4 + 8 * 8 + 32 + (partial ? crt_z_bytes(P) : 0);
 }
 
 // Last step of a CRT computed in blocks: per coefficient, v = round(sum of the blocks'

@@ -55,6 +55,16 @@ struct ChunkMap {
     int lcw;  // log2(cw)
 };
 
+// Prime blocks of one result-byte block of the tensor-core CRT, accumulated in TMEM within one
+// launch: block q holds primes j0[q] .. j0[q] + k[q] (kp[q] padded, kb[q] K bytes, B image b[q]
+// of this byte block), each tile's MMAs over the blocks in turn.  n = 0: one block, the
+// launch's DevPlan.
+struct CrtPrimeBlocks {
+    int n;
+    int j0[4], k[4], kp[4], kb[4];
+    const unsigned char* b[4];
+};
+
 __device__ __forceinline__ uint32_t chunk_pos_to_n(const DevPlan& P, const ChunkMap& C, uint32_t pos) {
     return ((pos >> C.lcw) << P.w2) + C.col0 + (pos & (C.cw - 1));
 }

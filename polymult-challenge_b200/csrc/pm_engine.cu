@@ -604,8 +604,7 @@ bool Engine::make_crt_blocks() {
     auto round_up = [](int x, int m) { return (x + m - 1) / m * m; };
     int kpb = std::min(plan_.KP, 128) & ~3;
     for (; kpb >= 4; kpb -= 4) {
-        DevPlan t = dp_;
-        t.KP = kpb;
+        DevPlan t = dp_;  // KP: the whole plan's 1/p table, which a byte-block launch stages
         t.crt_kbytes = round_up(4 * kpb, 32);
         t.crt_nrows = std::min(256, nrows_full);
         if (crt_tc_smem(t, true) <= smem_optin_) break;
@@ -643,6 +642,37 @@ bool Engine::make_crt_blocks() {
             crt_blocks_.push_back(b);
         }
     }
+    // group the blocks by result-byte block: one launch each, its prime blocks in TMEM
+    crt_byte_launches_.clear();
+    for (int v0 = 0; v0 < nrows_full; v0 += 256) {
+        CrtByteLaunch bl;
+        bl.dp = dp_;
+        bl.dp.crt_nrows = std::min(256, nrows_full - v0);
+        bl.dp.crt_kbytes = 0;
+        for (const CrtBlock& b : crt_blocks_) {
+            if (b.limb0 != v0 / 4) continue;
+            if (bl.pbs.n == 4) {
+                crt_byte_launches_.clear();
+                return true;
+            }
+            const int q = bl.pbs.n++;
+            bl.pbs.j0[q] = (int)b.j0;
+            bl.pbs.k[q] = b.dp.K;
+            bl.pbs.kp[q] = b.dp.KP;
+            bl.pbs.kb[q] = b.dp.crt_kbytes;
+            bl.pbs.b[q] = b.dp.crt_b;
+            bl.dp.crt_kbytes = std::max(bl.dp.crt_kbytes, b.dp.crt_kbytes);
+        }
+        bl.mode = v0 == 0 ? CRT_PARTIAL_FIRST : CRT_PARTIAL_ADD;
+        bl.limb0 = v0 / 4;
+        bl.add_s = v0 == 0;
+        bl.smem = crt_tc_smem(bl.dp, true);  // the whole plan's 1/p table
+        if (bl.pbs.n == 0 || bl.smem > smem_optin_) {
+            crt_byte_launches_.clear();
+            return true;
+        }
+        crt_byte_launches_.push_back(bl);
+    }
     return true;
 }
 
@@ -660,7 +690,9 @@ void Engine::reserve_crt_partials(size_t coeffs) {
 
 int Engine::kernel_launches_per_group() const {
     const int dec = dec_tc_ ? (int)dec_blocks_.size() : 1;
-    const int crt = crt_blocked_ ? (int)crt_blocks_.size() + 1 : 1;
+    const int crt = crt_blocked_
+                        ? (int)(crt_byte_launches_.empty() ? crt_blocks_.size() : crt_byte_launches_.size()) + 1
+                        : 1;
     // column passes of a, b and the inverse, and one row pass for both operands
     return 2 * dec + crt + (plan_.w1 > 0 ? 4 : 1);
 }
@@ -730,7 +762,7 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         const CrtPartial full{nullptr, nullptr, CRT_FULL, 0, 0};
         cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), smem_crt_, s, pdl, dp_, R, chunk_map(ch),
-                                 npos, nb, out, full),
+                                 npos, nb, out, full, CrtPrimeBlocks{}),
                    "launch k_crt_tc");
     } else if (crt_blocked_) {
         const size_t coeffs = (size_t)npos * nb;
@@ -739,12 +771,23 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
         float* sp = d_sp_ + poff;
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
-        for (const CrtBlock& b : crt_blocks_) {
-            const CrtPartial part{zp, sp, b.mode, b.limb0, b.add_s};
-            cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), b.smem, s, pdl, b.dp,
-                                     R + (size_t)b.j0 * plan_.N, chunk_map(ch), npos, nb, out, part),
-                       "launch k_crt_tc (block)");
-            pdl = true;  // each later launch follows the previous block's
+        if (!crt_byte_launches_.empty()) {
+            for (const CrtByteLaunch& bl : crt_byte_launches_) {
+                const CrtPartial part{zp, sp, bl.mode, bl.limb0, bl.add_s};
+                cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), bl.smem, s, pdl, bl.dp, R,
+                                         chunk_map(ch), npos, nb, out, part, bl.pbs),
+                           "launch k_crt_tc (byte block)");
+                pdl = true;  // each later launch follows the previous one
+            }
+        } else {
+            for (const CrtBlock& b : crt_blocks_) {
+                const CrtPartial part{zp, sp, b.mode, b.limb0, b.add_s};
+                cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), b.smem, s, pdl, b.dp,
+                                         R + (size_t)b.j0 * plan_.N, chunk_map(ch), npos, nb, out, part,
+                                         CrtPrimeBlocks{}),
+                           "launch k_crt_tc (block)");
+                pdl = true;  // each later launch follows the previous block's
+            }
         }
         const size_t fsmem = (size_t)TC_M * crt_zstride(plan_.L) * 4;
         cuda_check(launch_kernel(k_crt_finish, dim3((unsigned)((coeffs + TC_M - 1) / TC_M)), dim3(TC_M), fsmem, s,

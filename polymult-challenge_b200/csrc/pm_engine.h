@@ -159,6 +159,15 @@ class Engine {
         int mode = 0, limb0 = 0, add_s = 0;
         size_t smem = 0;
     };
+    // one launch per result-byte block with every prime block accumulated in TMEM (empty: one
+    // launch per (prime block, byte block), where a byte block would need more than 4)
+    struct CrtByteLaunch {
+        DevPlan dp;
+        CrtPrimeBlocks pbs{};
+        int mode = 0, limb0 = 0, add_s = 0;
+        size_t smem = 0;
+    };
+    std::vector<CrtByteLaunch> crt_byte_launches_;
     bool make_crt_blocks();
     void reserve_crt_partials(size_t coeffs);
     void upload_tables();

@@ -75,7 +75,7 @@ struct CrtPartial {
     int add_s;     // whether this launch adds its sum of y_j / p_j (once per prime block)
 };
 __global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
-                         CrtPartial part);
+                         CrtPartial part, CrtPrimeBlocks pbs);
 __global__ void k_crt_finish(DevPlan P, const uint32_t* zp, const float* sp, uint32_t total, uint32_t* out);
 constexpr int RNS_TC_THREADS = 640;  // 4 loader warps + 16 epilogue warps (4 lane quarters x 2 prime halves x 2 column sets)
 constexpr int CRT_TC_THREADS = 512;  // 256 producers + 256 epilogue threads, two per coefficient each
