@@ -60,9 +60,10 @@ struct ChunkMap {
 // of this byte block), each tile's MMAs over the blocks in turn.  n = 0: one block, the
 // launch's DevPlan.
 struct CrtPrimeBlocks {
+    static constexpr int MAX = 8;
     int n;
-    int j0[4], k[4], kp[4], kb[4];
-    const unsigned char* b[4];
+    int j0[MAX], k[MAX], kp[MAX], kb[MAX];
+    const unsigned char* b[MAX];
 };
 
 __device__ __forceinline__ uint32_t chunk_pos_to_n(const DevPlan& P, const ChunkMap& C, uint32_t pos) {

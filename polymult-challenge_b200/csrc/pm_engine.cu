@@ -651,7 +651,7 @@ bool Engine::make_crt_blocks() {
         bl.dp.crt_kbytes = 0;
         for (const CrtBlock& b : crt_blocks_) {
             if (b.limb0 != v0 / 4) continue;
-            if (bl.pbs.n == 4) {
+            if (bl.pbs.n == CrtPrimeBlocks::MAX) {
                 crt_byte_launches_.clear();
                 return true;
             }

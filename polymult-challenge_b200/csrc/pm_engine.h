@@ -160,7 +160,8 @@ class Engine {
         size_t smem = 0;
     };
     // one launch per result-byte block with every prime block accumulated in TMEM (empty: one
-    // launch per (prime block, byte block), where a byte block would need more than 4)
+    // launch per (prime block, byte block), where a byte block would need more than
+    // CrtPrimeBlocks::MAX)
     struct CrtByteLaunch {
         DevPlan dp;
         CrtPrimeBlocks pbs{};
