@@ -498,7 +498,12 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     const int K = P.K, KP = P.KP, L = P.L, kb = P.crt_kbytes, nrows_b = P.crt_nrows;
     const int zl = crt_zl(L), zs = crt_zstride(L);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t AS = tmem_cols_for(nrows_b);     // columns per accumulator (<= 256)
+    const uint32_t AS = tmem_cols_for(nrows_b);     // columns per accumulator (<= 512)
+    // accumulators: two (tile i in i & 1, so that its epilogue overlaps tile i + 1's MMAs), or
+    // one wide one (more than 256 result bytes); buffer of tile i and how often it was used before
+    const int nbuf = 2 * AS <= 512 ? 2 : 1;
+    auto buf_of = [&](uint32_t t) { return nbuf == 2 ? (int)(t & 1) : 0; };
+    auto use_of = [&](uint32_t t) { return nbuf == 2 ? t >> 1 : t; };
     const uint32_t tiles_per_batch = (npos + TC_M - 1) / TC_M;
     const uint32_t ntiles = tiles_per_batch * nbatch;
     const uint32_t sbo = 8u * (uint32_t)kb;
@@ -515,7 +520,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         if (pbs.n == 0) bulk_g2s_all(S.b, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);  // else per block
     }
     for (int j = threadIdx.x; j < KP; j += blockDim.x) S.rcp[j] = P.rcp[j];
-    if (warp == 0) tmem_alloc(S.slot, 2 * AS);
+    if (warp == 0) tmem_alloc(S.slot, nbuf * AS);
     // the prologue above reads only the plan's constant tables; R, the partial buffers and the
     // output come after the previous kernel in the stream
     pdl_wait();
@@ -539,7 +544,8 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         // constant times gamma_j = crt_c_j 2^-32, the CRT's per-prime factor.  They stay
         // unreduced in [0, 2p_j): with y'_j = y_j + d_j p_j, sum y'_j M/p_j and
         // v' = round(sum y'_j / p_j) both grow by (sum d_j) M, so z = sum y'_j Q_j + v' T_1 is
-        // the same residue mod q, v' <= 2K - 1 <= 255 still fits A's v byte, and the fractional
+        // the same residue mod q, v' <= 2K - 1 still fits A's v byte (K <= 128; the prime-block
+        // form gives v' a second byte), and the fractional
         // part of the sum, which the exactness check reads, is unchanged.  The padding primes
         // K..KP-1 meet zero B columns (but for A's v column, written after them) and 1/p = 0.
         // With prime blocks (pbs.n > 0) a tile runs the blocks in turn: each block's residues into
@@ -552,7 +558,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         uint32_t i = 0, seq = 0;  // seq: prime-block MMA groups so far (npb per tile)
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(1, CRT_PROD_THREADS, *S.abort != 0)) break;
-            const int b = (int)(i & 1);
+            const int b = buf_of(i);
             const uint32_t bt = tile / tiles_per_batch;
             const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
             // positions past the end of the batch repeat the tile's first one: their A rows and
@@ -577,7 +583,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                         b_par = seq & 1;
                     }
                 } else if (i > 0) {
-                    wait_or_abort(mma_done + ((i - 1) & 1), ((i - 1) >> 1) & 1, S.abort);
+                    wait_or_abort(mma_done + buf_of(i - 1), use_of(i - 1) & 1, S.abort);
                 }
                 // every residue of this thread's primes straight into its A row with 4-byte async
                 // copies: no register staging, the whole tile in flight at once (register batches
@@ -606,7 +612,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 if (last) {
                     // the epilogue of tile i - 2 must have read partial sums [b] (it arrives on
                     // acc_empty[b] after that)
-                    if (i > 1) wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
+                    if (use_of(i) > 0) wait_or_abort(acc_empty + b, (use_of(i) - 1) & 1, S.abort);
                     S.spart[(b * 2 + h) * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
                     if (part.mode == CRT_FULL) {
                         // v = round(sum y_j / p_j) (|x| < M/8 keeps the sum within 1/8 of an integer;
@@ -617,8 +623,13 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                             const float vf = rintf(sum);
                             if ((uint32_t)m < npos - pos0 && fabsf(sum - vf) > 0.25f)
                                 flag_error(P.status, DEV_ERR_CRT_BOUND);
-                            arow[(size_t)(P.crt_kv >> 4) * 128 + (P.crt_kv & 15)] =
-                                (unsigned char)min(max((int)vf, 0), 2 * K - 1);
+                            // the v column, in the last prime block's K bytes; with prime blocks
+                            // (K > 128) v may pass 255 and takes a second column: v / 256 against
+                            // 256 T_1
+                            const int v = min(max((int)vf, 0), 2 * K - 1);
+                            const int kvl = P.crt_kv - (pbs.n ? 4 * pbs.j0[npb - 1] : 0);
+                            arow[(size_t)(kvl >> 4) * 128 + (kvl & 15)] = (unsigned char)(v & 255);
+                            if (pbs.n) arow[(size_t)((kvl + 1) >> 4) * 128 + ((kvl + 1) & 15)] = (unsigned char)(v >> 8);
                         }
                     }
                 }
@@ -632,12 +643,17 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                         if (ok) b_pend = false;
                         // the block's first MMA starts the accumulator afresh: tile i - 2's
                         // epilogue must have read it
-                        if (ok && pb == 0 && i > 1) ok = wait_or_abort(acc_empty + b, ((i >> 1) - 1) & 1, S.abort);
+                        if (ok && pb == 0 && use_of(i) > 0)
+                            ok = wait_or_abort(acc_empty + b, (use_of(i) - 1) & 1, S.abort);
                     }
                     if (ok) {
                         tc_fence_after();
                         const uint32_t acc = tmem + (uint32_t)b * AS;
-                        issue_gemm_rows(acc, smem_addr(S.a), smem_addr(S.b), 0, nrows_b, kbb, pb > 0);
+                        // MMA N is at most 256: a wider accumulator takes two row ranges of B
+                        const int n_lo = min(nrows_b, 256);
+                        issue_gemm_rows(acc, smem_addr(S.a), smem_addr(S.b), 0, n_lo, kbb, pb > 0);
+                        if (nrows_b > 256)
+                            issue_gemm_rows(acc + 256, smem_addr(S.a), smem_addr(S.b), 256, nrows_b - 256, kbb, pb > 0);
                         if (pbs.n) {
                             umma_commit(ab_free);
                             ++ab_commits;
@@ -661,14 +677,14 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(2, CRT_EPI_THREADS, *S.abort != 0)) break;
-            const int b = (int)(i & 1);
+            const int b = buf_of(i);
             const uint32_t bt = tile / tiles_per_batch;
             const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
             const int cnt = (int)min((uint32_t)TC_M, npos - pos0);
             const bool valid = m < cnt;
             // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
-            const bool got = __all_sync(0xffffffffu, wait_or_abort(v_ready + b, (i >> 1) & 1, S.abort) &&
-                                                         wait_or_abort(mma_done + b, (i >> 1) & 1, S.abort));
+            const bool got = __all_sync(0xffffffffu, wait_or_abort(v_ready + b, use_of(i) & 1, S.abort) &&
+                                                         wait_or_abort(mma_done + b, use_of(i) & 1, S.abort));
             tc_fence_after();
             const size_t gpos = (size_t)bt * npos + pos0;  // first coefficient of the tile in the partial buffers
             if (part.mode != CRT_FULL && part.add_s && hf == 0 && valid) {
@@ -808,13 +824,13 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
         flag_error(P.status, DEV_ERR_WAIT);
         // copies and MMAs still in flight must land before this CTA's memory goes away
         if (!b_seen) mbar_wait_bounded(bar_b, 0);
-        if (issued) mbar_wait_bounded(mma_done + ((issued - 1) & 1), ((issued - 1) >> 1) & 1);
+        if (issued) mbar_wait_bounded(mma_done + buf_of(issued - 1), use_of(issued - 1) & 1);
         if (b_pend) mbar_wait_bounded(bar_b, b_par);
     }
     // the last prime block's ab_free arrival (its MMAs are complete: the epilogue waited for them)
     if (threadIdx.x == 0 && ab_commits) mbar_wait_bounded(ab_free, (ab_commits - 1) & 1);
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, 2 * AS);
+    if (warp == 0) tmem_dealloc(tmem, nbuf * AS);
 }
 
 size_t rns_tc_smem(const DevPlan& P) {

@@ -282,6 +282,7 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
         const bool dec_fits = make_dec_blocks();
         const bool crt_fits = crt_tc_smem(dp_) <= smem_optin_ && plan_.KP <= 128 && dp_.crt_nrows <= 256;
         const bool crt_blocks = !crt_fits && dec_fits && make_crt_blocks();
+        if (crt_blocks) make_crt_wide();
         if (gemm_request == GEMM_TENSOR && !(dec_fits && (crt_fits || crt_blocks)))
             throw Unsupported("tensor-core GEMM form does not cover this point (shared memory / TMEM)");
         if (gemm_request == GEMM_MIXED && !dec_fits)
@@ -676,6 +677,69 @@ bool Engine::make_crt_blocks() {
     return true;
 }
 
+// The CRT of a point with more than 128 primes and at most 512 result bytes in one launch: one
+// TMEM accumulator holds every result byte of a tile (its epilogue no longer overlaps the next
+// tile's MMAs), the tile's prime blocks accumulate into it in turn, and the epilogue is the
+// single-block one (v column, fold, -q) -- no partial integers, no k_crt_finish.  Each prime
+// block's B image covers all result rows and the block's own K bytes; the last block's also
+// the v column (its K bytes extended to reach it).  False where the blocks or shared memory do
+// not allow it.
+bool Engine::make_crt_wide() {
+    crt_wide_ok_ = false;
+    const int nrows_full = plan_.crt_gemm.n_rows, kb_full = plan_.crt_gemm.k_bytes;
+    if (nrows_full > 512 || tmem_cols_for(nrows_full) > 512) return false;
+    auto round_up = [](int x, int m) { return (x + m - 1) / m * m; };
+    int kpb = std::min(plan_.KP, 128) & ~3;
+    for (; kpb >= 4; kpb -= 4) {
+        DevPlan t = dp_;
+        t.crt_kbytes = round_up(4 * kpb + 32, 32);  // room for the last block's v column
+        t.crt_nrows = nrows_full;
+        if (crt_tc_smem(t, false) <= smem_optin_) break;
+    }
+    if (kpb < 4) return false;
+    CrtByteLaunch w;
+    w.dp = dp_;
+    w.dp.crt_nrows = nrows_full;
+    w.dp.crt_kbytes = 0;
+    std::vector<std::pair<int, int>> blocks;  // (j0, count)
+    for (int j0 = 0; j0 < plan_.K; j0 += kpb) blocks.push_back({j0, std::min(kpb, plan_.K - j0)});
+    if ((int)blocks.size() > CrtPrimeBlocks::MAX) return false;
+    for (size_t q = 0; q < blocks.size(); ++q) {
+        const int j0 = blocks[q].first, cnt = blocks[q].second, kp = (cnt + 3) & ~3;
+        const bool last = q + 1 == blocks.size();
+        // v = round(sum y'_j / p_j) <= 2K - 1 needs two bytes once K > 128: A's v column kvl
+        // takes v mod 256 against T_1's bytes, column kvl + 1 takes v / 256 against T_1's bytes
+        // one result byte up (256 T_1), so that the MMA adds v T_1
+        const int kvl = plan_.crt_kv - 4 * j0;  // the v column in this block's K bytes (last block)
+        const int kb = round_up(last ? std::max(4 * kp, kvl + 2) : 4 * kp, 32);
+        std::vector<uint8_t> img((size_t)nrows_full * kb, 0);
+        for (int v = 0; v < nrows_full; ++v)
+            for (int kbyte = 0; kbyte < kb; ++kbyte) {
+                const int fk = 4 * j0 + kbyte;
+                if (last && kbyte == kvl + 1) {
+                    if (v > 0) img[umma_kmajor_offset(v, kbyte, kb)] =
+                                   plan_.crt_b[umma_kmajor_offset(v - 1, plan_.crt_kv, kb_full)];
+                } else if (fk < kb_full && (kbyte < 4 * kp || (last && kbyte == kvl))) {
+                    // the block's own primes, and the v column in the last block
+                    img[umma_kmajor_offset(v, kbyte, kb)] = plan_.crt_b[umma_kmajor_offset(v, fk, kb_full)];
+                }
+            }
+        const int n = w.pbs.n++;
+        w.pbs.j0[n] = j0;
+        w.pbs.k[n] = cnt;
+        w.pbs.kp[n] = kp;
+        w.pbs.kb[n] = kb;
+        w.pbs.b[n] = dev_upload(dev_allocs_, img, &table_bytes_);
+        w.dp.crt_kbytes = std::max(w.dp.crt_kbytes, kb);
+    }
+    w.mode = CRT_FULL;
+    w.smem = crt_tc_smem(w.dp, false);
+    if (w.smem > smem_optin_) return false;
+    crt_wide_ = w;
+    crt_wide_ok_ = true;
+    return true;
+}
+
 void Engine::reserve_crt_partials(size_t coeffs) {
     if (!crt_blocked_ || coeffs <= partial_coeffs_) return;
     if (d_zp_) cudaFree(d_zp_);
@@ -690,9 +754,9 @@ void Engine::reserve_crt_partials(size_t coeffs) {
 
 int Engine::kernel_launches_per_group() const {
     const int dec = dec_tc_ ? (int)dec_blocks_.size() : 1;
-    const int crt = crt_blocked_
-                        ? (int)(crt_byte_launches_.empty() ? crt_blocks_.size() : crt_byte_launches_.size()) + 1
-                        : 1;
+    const int crt = !crt_blocked_ || crt_wide_ok_
+                        ? 1
+                        : (int)(crt_byte_launches_.empty() ? crt_blocks_.size() : crt_byte_launches_.size()) + 1;
     // column passes of a, b and the inverse, and one row pass for both operands
     return 2 * dec + crt + (plan_.w1 > 0 ? 4 : 1);
 }
@@ -764,6 +828,13 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
         cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), smem_crt_, s, pdl, dp_, R, chunk_map(ch),
                                  npos, nb, out, full, CrtPrimeBlocks{}),
                    "launch k_crt_tc");
+    } else if (crt_blocked_ && crt_wide_ok_) {
+        const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
+        const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
+        const CrtPartial full{nullptr, nullptr, CRT_FULL, 0, 0};
+        cuda_check(launch_kernel(k_crt_tc, dim3(grid), dim3(CRT_TC_THREADS), crt_wide_.smem, s, pdl, crt_wide_.dp, R,
+                                 chunk_map(ch), npos, nb, out, full, crt_wide_.pbs),
+                   "launch k_crt_tc (wide)");
     } else if (crt_blocked_) {
         const size_t coeffs = (size_t)npos * nb;
         if (poff + coeffs > partial_coeffs_) throw Unsupported("blocked CRT: partial buffers reserved for fewer coefficients");

@@ -169,6 +169,11 @@ class Engine {
         size_t smem = 0;
     };
     std::vector<CrtByteLaunch> crt_byte_launches_;
+    // all result bytes of a wide point in one accumulator of up to 512 TMEM columns (no double
+    // buffering), every prime block accumulated, the full CRT in one launch: no partial integers
+    CrtByteLaunch crt_wide_;
+    bool crt_wide_ok_ = false;
+    bool make_crt_wide();
     bool make_crt_blocks();
     void reserve_crt_partials(size_t coeffs);
     void upload_tables();
