@@ -225,9 +225,11 @@ static_assert(DEC_EPI_THREADS % TC_M == 0, "whole warps per lane quarter");
 
 __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const uint32_t* __restrict__ src, ChunkMap C,
                                                               uint32_t npos, uint32_t nbatch, uint32_t* __restrict__ R,
-                                                              int use_bulk) {
+                                                              int use_bulk, int ring) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int L = P.L, kb = P.dec_kbytes, nrows_b = P.dec_nrows;
+    // ring: raw tiles in flight (2: prefetched two tiles ahead; 1: one slot, refilled once its
+    // tile is relaid, which frees shared memory for wider prime blocks)
     const int KH = dec_half_primes(P.KP);                 // primes of half 0
     const int n0 = 4 * KH, n1 = nrows_b - n0;              // MMA N of the halves
     const uint32_t col1 = dec_half1_col(n0);               // TMEM column of half 1
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
     unsigned char* a_s = b_s + (size_t)nrows_b * kb;
     uint32_t* raw_s = reinterpret_cast<uint32_t*>(a_s + (size_t)TC_M * kb);
     const size_t raw_words = (size_t)TC_M * L;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(raw_s + 2 * raw_words);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(raw_s + ring * raw_words);
     uint64_t *bar_b = bars, *bar_raw = bars + 1, *mma_done = bars + 3, *acc_empty = bars + 5;
     uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 7);
     volatile int* abort_f = reinterpret_cast<volatile int*>(slot + 1);
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
     // the previous kernel in the stream
     pdl_wait();
     if (threadIdx.x == 0 && use_bulk)
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < ring; ++k) {
             const uint32_t t = blockIdx.x + k * gridDim.x;
             if (t < ntiles) {
                 int cnt;
@@ -289,7 +291,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
     bool b_seen = false;
     uint32_t raw_pending = 0, raw_par = 0;
     if (threadIdx.x == 0 && use_bulk)
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < ring; ++k)
             if (blockIdx.x + k * gridDim.x < ntiles) raw_pending |= 1u << k;  // parity 0
 
     if (threadIdx.x < DEC_LOAD_THREADS) {
@@ -299,12 +301,13 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(1, DEC_LOAD_THREADS, *abort_f != 0)) break;
-            const int buf = (int)(i & 1);
+            const int buf = ring == 2 ? (int)(i & 1) : 0;  // raw ring slot
             int cnt;
             const uint32_t* s = tile_src(tile, &cnt);
             uint32_t* raw = raw_s + buf * raw_words;
             if (use_bulk) {
-                if (wait_or_abort(bar_raw + buf, (i >> 1) & 1, abort_f) && threadIdx.x == 0) raw_pending &= ~(1u << buf);
+                if (wait_or_abort(bar_raw + buf, (ring == 2 ? i >> 1 : i) & 1, abort_f) && threadIdx.x == 0)
+                    raw_pending &= ~(1u << buf);
             } else {
                 for (int w = threadIdx.x; w < cnt * L; w += DEC_LOAD_THREADS) raw[w] = __ldg(s + w);
             }
@@ -341,13 +344,14 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
             fence_smem_to_async();
             named_sync(1, DEC_LOAD_THREADS);
             if (threadIdx.x == 0) {
-                const uint32_t nxt = tile + 2 * gridDim.x;
+                const uint32_t nxt = tile + (uint32_t)ring * gridDim.x;
                 if (use_bulk && nxt < ntiles) {  // the ring slot was just consumed
                     int c2;
                     const uint32_t* s2 = tile_src(nxt, &c2);
                     bulk_g2s_all(raw, s2, (uint32_t)c2 * L * 4, bar_raw + buf);
                     raw_pending |= 1u << buf;
-                    raw_par = (raw_par & ~(1u << buf)) | ((((i + 2) >> 1) & 1u) << buf);
+                    const uint32_t use = ring == 2 ? (i + 2) >> 1 : i + 1;  // the slot's next use
+                    raw_par = (raw_par & ~(1u << buf)) | ((use & 1u) << buf);
                 }
                 bool ok = *abort_f == 0;
                 if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, abort_f);
@@ -833,8 +837,8 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     if (warp == 0) tmem_dealloc(tmem, nbuf * AS);
 }
 
-size_t rns_tc_smem(const DevPlan& P) {
-    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + 2 * (size_t)TC_M * P.L * 4 + 7 * 8 + 8 +
+size_t rns_tc_smem(const DevPlan& P, int ring) {
+    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + (size_t)ring * TC_M * P.L * 4 + 7 * 8 + 8 +
            (size_t)P.KP * 8;
 }
 

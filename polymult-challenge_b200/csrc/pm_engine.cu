@@ -568,16 +568,30 @@ void Engine::setup_host_pipeline() {
 // A block's B operand is a contiguous slice of the full image (rows 4j + t, 4 j0 a multiple
 // of 8); its kernel sees K = the block's primes, p / pinv from j0, and writes residue rows
 // j0.. of the full arrays.  False if no block fits.
+//
+// A point that needs several blocks takes a one-tile raw ring where that makes the blocks wider
+// (fewer blocks: each re-reads the operand), e.g. 84 instead of 52 primes at W = 3000.
 bool Engine::make_dec_blocks() {
     dec_blocks_.clear();
-    int kpb = std::min(plan_.KP, 128) & ~3;
-    for (; kpb >= 4; kpb -= 4) {
-        DevPlan t = dp_;
-        t.KP = kpb;
-        t.dec_nrows = 4 * kpb;
-        if (rns_tc_smem(t) <= smem_optin_) break;
-    }
+    auto block_primes = [&](int ring) {
+        int k = std::min(plan_.KP, 128) & ~3;
+        for (; k >= 4; k -= 4) {
+            DevPlan t = dp_;
+            t.KP = k;
+            t.dec_nrows = 4 * k;
+            if (rns_tc_smem(t, ring) <= smem_optin_) break;
+        }
+        return k;
+    };
+    int kpb = block_primes(2), ring = 2;
     if (kpb < 4) return false;
+    if (kpb < plan_.K) {
+        const int kpb1 = block_primes(1);
+        if ((plan_.K + kpb1 - 1) / kpb1 < (plan_.K + kpb - 1) / kpb) {
+            kpb = kpb1;
+            ring = 1;
+        }
+    }
     for (int j0 = 0; j0 < plan_.K; j0 += kpb) {
         DecBlock b;
         b.j0 = (uint32_t)j0;
@@ -589,7 +603,8 @@ bool Engine::make_dec_blocks() {
         b.dp.dec_b += (size_t)4 * j0 * dp_.dec_kbytes;
         b.dp.dec_b_ra += (size_t)4 * j0 * dp_.dec_kbytes;
         b.dp.dec_nrows = 4 * b.dp.KP;
-        b.smem = rns_tc_smem(b.dp);
+        b.ring = ring;
+        b.smem = rns_tc_smem(b.dp, ring);
         dec_blocks_.push_back(b);
     }
     return true;
@@ -787,7 +802,7 @@ void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R,
             DevPlan d = b.dp;
             if (scaled) d.dec_b = d.dec_b_ra;
             cuda_check(launch_kernel(k_rns_tc, dim3(grid), dim3(RNS_TC_THREADS), b.smem, s, pdl, d, src,
-                                     chunk_map(ch), npos, nb, R + (size_t)b.j0 * plan_.N, bulk),
+                                     chunk_map(ch), npos, nb, R + (size_t)b.j0 * plan_.N, bulk, b.ring),
                        "launch k_rns_tc");
             pdl = true;  // the next prime block follows this launch
         }

@@ -150,6 +150,7 @@ class Engine {
         DevPlan dp;        // the block's view of the plan (primes j0 .. j0 + dp.K)
         uint32_t j0 = 0;
         size_t smem = 0;
+        int ring = 2;      // raw input tiles in flight
     };
     bool make_dec_blocks();
     // (prime block, result-byte block) launches of a CRT too large for one tile

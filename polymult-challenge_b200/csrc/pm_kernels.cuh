@@ -61,8 +61,9 @@ size_t crt_plain_smem(const DevPlan& P);
 
 // ---- tensor-core (tcgen05 kind::i8) RNS decomposition and CRT (k_tc.cu)
 constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
+// ring: raw input tiles in flight (1 or 2; rns_tc_smem counts them)
 __global__ void k_rns_tc(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* R,
-                         int use_bulk);
+                         int use_bulk, int ring);
 // A CRT over more primes than one tile holds runs as a sequence of k_crt_tc launches over
 // (prime block, result-byte block) pairs that accumulate exact per-coefficient partial integers
 // (zl = L + 3 limbs each) and partial sums of y_j / p_j, then k_crt_finish.
@@ -79,7 +80,7 @@ __global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos
 __global__ void k_crt_finish(DevPlan P, const uint32_t* zp, const float* sp, uint32_t total, uint32_t* out);
 constexpr int RNS_TC_THREADS = 640;  // 4 loader warps + 16 epilogue warps (4 lane quarters x 2 prime halves x 2 column sets)
 constexpr int CRT_TC_THREADS = 512;  // 256 producers + 256 epilogue threads, two per coefficient each
-size_t rns_tc_smem(const DevPlan& P);
+size_t rns_tc_smem(const DevPlan& P, int ring = 2);
 size_t crt_tc_smem(const DevPlan& P, bool partial = false);
 // TMEM columns to allocate: a power of two >= max(32, n)
 __host__ __device__ inline uint32_t tmem_cols_for(int n) {
