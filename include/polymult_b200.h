@@ -105,7 +105,10 @@ int pm_time_stages(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, ui
  * return PM_ERR_INVALID.  Asynchronous on `stream`; pm_sync() reports device-side checks.
  * All calls share the scratch array: calls that overlap on the GPU race, so serialise them.
  * The first call on a device looks up the array's device address; make it before any stream
- * capture.  The context must come from an earlier pm_init (which does allocate). */
+ * capture.  pm_free forgets that address (free every context of a device before a
+ * cudaDeviceReset, after which it would be stale).  The context must come from an earlier
+ * pm_init (which does allocate).  Like the other entry points that run a context, it leaves the
+ * caller's current device as it found it; errors map as pm_run_device's do. */
 int pm_run_device_static(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream);
 
 /* ---- Batches of multiplications of uneven points.  No reference counterpart: the reference
@@ -236,11 +239,36 @@ const char* pm_last_error(void);
 int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int32_t* K_out);
 
 /* Host-only: stress test of the thread pool that stages pm_run's pageable operands.  Creates
- * `pools` pools of `workers` threads and runs `runs` task sets on each (task counts 1..64,
- * varying when `vary`, else 64 every time), counting task sets where a task ran other than once
- * or was still running when the set returned.  *failures gets that count (0 expected).  No GPU
- * needed. */
+ * `pools` pools of `workers` threads and runs `runs` task sets on each, counting task sets where
+ * a task ran other than once or was still running when the set returned.  *failures gets that
+ * count (0 expected).  `vary` bit 0: task counts 1..64 instead of 64 every time; bit 1: workers
+ * park between task sets (20 us idle limit, a 300 us pause before every third set) so that each
+ * set has to wake them.  No GPU needed. */
 int pm_selftest_host_pool(uint32_t pools, uint32_t runs, uint32_t workers, int vary, uint64_t* failures);
+
+/* Test hook, host-only: after `skip` more residue-scratch allocations of any context (each
+ * context's scratch is two arrays), the next `n` fail as if cudaMalloc had run out of device
+ * memory; the calls that needed them return PM_ERR_CUDA and the context holds no scratch until
+ * a later call allocates it again.  Lets tests drive the allocation-failure path without
+ * exhausting a shared GPU.  (0, 0) switches the injection off. */
+void pm_test_fail_scratch_allocs(int skip, int n);
+
+/* Test hook: writes `bits` (PM_DEVICE_* below) into the context's device status word, as a
+ * failed device-side check would; the next pm_sync or pm_run then reports PM_ERR_DEVICE and
+ * clears the word.  Waits for the context's device work first. */
+int pm_test_set_status(pm_context* ctx, uint32_t bits);
+#define PM_DEVICE_CRT_BOUND 1u /* fp32 CRT estimate not within 1/4 of an integer (|x| < M/8 violated) */
+#define PM_DEVICE_FOLD 2u      /* CRT value above its bound after the folds */
+#define PM_DEVICE_WAIT 4u      /* an mbarrier wait of a tensor-core kernel ran out */
+
+/* No reference counterpart (the reference's waits are host-side, solve.cu:814-816): the bounded
+ * mbarrier waits of the tensor-core kernels, made to run out.  One block of 64 threads waits
+ * with a limit of `limit_clocks` (1 .. 2e9) on an mbarrier that nothing arrives on, as the
+ * kernels' waits do (one thread alone, and a warp sharing an abort flag); each must give up and
+ * report PM_DEVICE_WAIT in *status_out.  Then the phase is completed and every thread's wait must
+ * succeed (bit 8 of *status_out otherwise).  Nothing is in flight while they wait, so the context
+ * stays usable.  Synchronous. */
+int pm_selftest_wait(int device, uint64_t limit_clocks, uint32_t* status_out);
 
 #ifdef __cplusplus
 }

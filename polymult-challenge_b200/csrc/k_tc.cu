@@ -47,11 +47,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for phase `parity` of `bar`; false after about one second of clocks.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Waits for phase `parity` of `bar`; false once `limit` clocks have passed (the plan's
+// wait_clocks: 2e9, about one second).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > 2000000000ll) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -185,12 +186,12 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 
 // Bounded wait that also gives up once another thread has set *abort; sets *abort itself
-// when its own limit (about one second of clocks) runs out.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+// when its own limit of `limit` clocks runs out.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort, long long limit) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
         if (*abort) return false;
-        if (clock64() - t0 > 2000000000ll) {
+        if (clock64() - t0 > limit) {
             *abort = 1;
             return false;
         }
@@ -306,13 +307,13 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
             const uint32_t* s = tile_src(tile, &cnt);
             uint32_t* raw = raw_s + buf * raw_words;
             if (use_bulk) {
-                if (wait_or_abort(bar_raw + buf, (ring == 2 ? i >> 1 : i) & 1, abort_f) && threadIdx.x == 0)
+                if (wait_or_abort(bar_raw + buf, (ring == 2 ? i >> 1 : i) & 1, abort_f, P.wait_clocks) && threadIdx.x == 0)
                     raw_pending &= ~(1u << buf);
             } else {
                 for (int w = threadIdx.x; w < cnt * L; w += DEC_LOAD_THREADS) raw[w] = __ldg(s + w);
             }
             // the previous tile's MMAs must have read A (mma_done of its last half)
-            if (i > 0) wait_or_abort(mma_done + (nhalves - 1), (i - 1) & 1, abort_f);
+            if (i > 0) wait_or_abort(mma_done + (nhalves - 1), (i - 1) & 1, abort_f, P.wait_clocks);
             named_sync(1, DEC_LOAD_THREADS);  // raw tile visible to the whole group
             // re-layout: thread = row mm; 16-byte group g = limbs 4g..4g+3 (zero past L or past
             // cnt).  The full groups unpredicated and unrolled, so that several groups' loads are
@@ -354,9 +355,9 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                     raw_par = (raw_par & ~(1u << buf)) | ((use & 1u) << buf);
                 }
                 bool ok = *abort_f == 0;
-                if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, abort_f);
+                if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, abort_f, P.wait_clocks);
                 for (int h = 0; h < nhalves && ok; ++h) {
-                    if (i > 0) ok = wait_or_abort(acc_empty + h, (i - 1) & 1, abort_f);
+                    if (i > 0) ok = wait_or_abort(acc_empty + h, (i - 1) & 1, abort_f, P.wait_clocks);
                     if (!ok) break;
                     tc_fence_after();
                     if (h == 0) issue_gemm_rows(tmem, smem_addr(a_s), smem_addr(b_s), 0, n0, kb);
@@ -388,7 +389,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
             // half 1 is read out
             for (int half = 0; half < nhalves; ++half) {
                 // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
-                const bool got = __all_sync(0xffffffffu, wait_or_abort(mma_done + half, i & 1, abort_f));
+                const bool got = __all_sync(0xffffffffu, wait_or_abort(mma_done + half, i & 1, abort_f, P.wait_clocks));
                 tc_fence_after();
                 const int j0 = half ? KH : 0;
                 const int cols = half ? n1 : n0;
@@ -446,10 +447,10 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
     if (threadIdx.x == 0 && *abort_f) {
         flag_error(P.status, DEV_ERR_WAIT);
         // copies and MMAs still in flight must land before this CTA's memory goes away
-        if (!b_seen) mbar_wait_bounded(bar_b, 0);
+        if (!b_seen) mbar_wait_bounded(bar_b, 0, P.wait_clocks);
         for (int k = 0; k < 2; ++k)
-            if (raw_pending & (1u << k)) mbar_wait_bounded(bar_raw + k, (raw_par >> k) & 1u);
-        if (last_commit >= 0) mbar_wait_bounded(mma_done + last_commit, last_commit_par);
+            if (raw_pending & (1u << k)) mbar_wait_bounded(bar_raw + k, (raw_par >> k) & 1u, P.wait_clocks);
+        if (last_commit >= 0) mbar_wait_bounded(mma_done + last_commit, last_commit_par, P.wait_clocks);
     }
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, ncols);
@@ -580,14 +581,14 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 const uint32_t* rp = rtile + (size_t)(j0b + 4 * g0) * N;
                 // the previous MMA group must have read A (and B) before they are overwritten
                 if (pbs.n) {
-                    if (seq > 0) wait_or_abort(ab_free, (seq - 1) & 1, S.abort);
+                    if (seq > 0) wait_or_abort(ab_free, (seq - 1) & 1, S.abort, P.wait_clocks);
                     if (threadIdx.x == 0) {
                         bulk_g2s_all(S.b, pbs.b[pb], (uint32_t)((size_t)nrows_b * kbb), bar_b);
                         b_pend = true;
                         b_par = seq & 1;
                     }
                 } else if (i > 0) {
-                    wait_or_abort(mma_done + buf_of(i - 1), use_of(i - 1) & 1, S.abort);
+                    wait_or_abort(mma_done + buf_of(i - 1), use_of(i - 1) & 1, S.abort, P.wait_clocks);
                 }
                 // every residue of this thread's primes straight into its A row with 4-byte async
                 // copies: no register staging, the whole tile in flight at once (register batches
@@ -616,7 +617,7 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 if (last) {
                     // the epilogue of tile i - 2 must have read partial sums [b] (it arrives on
                     // acc_empty[b] after that)
-                    if (use_of(i) > 0) wait_or_abort(acc_empty + b, (use_of(i) - 1) & 1, S.abort);
+                    if (use_of(i) > 0) wait_or_abort(acc_empty + b, (use_of(i) - 1) & 1, S.abort, P.wait_clocks);
                     S.spart[(b * 2 + h) * TC_M + m] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
                     if (part.mode == CRT_FULL) {
                         // v = round(sum y_j / p_j) (|x| < M/8 keeps the sum within 1/8 of an integer;
@@ -641,14 +642,14 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 named_sync(1, CRT_PROD_THREADS);
                 if (threadIdx.x == 0) {
                     bool ok = *S.abort == 0;
-                    if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, S.abort);
+                    if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, S.abort, P.wait_clocks);
                     if (ok && pbs.n) {
-                        ok = wait_or_abort(bar_b, seq & 1, S.abort);
+                        ok = wait_or_abort(bar_b, seq & 1, S.abort, P.wait_clocks);
                         if (ok) b_pend = false;
                         // the block's first MMA starts the accumulator afresh: tile i - 2's
                         // epilogue must have read it
                         if (ok && pb == 0 && use_of(i) > 0)
-                            ok = wait_or_abort(acc_empty + b, (use_of(i) - 1) & 1, S.abort);
+                            ok = wait_or_abort(acc_empty + b, (use_of(i) - 1) & 1, S.abort, P.wait_clocks);
                     }
                     if (ok) {
                         tc_fence_after();
@@ -687,8 +688,8 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
             const int cnt = (int)min((uint32_t)TC_M, npos - pos0);
             const bool valid = m < cnt;
             // warp-uniform: tcgen05.ld is executed by all lanes of a warp or by none
-            const bool got = __all_sync(0xffffffffu, wait_or_abort(v_ready + b, use_of(i) & 1, S.abort) &&
-                                                         wait_or_abort(mma_done + b, use_of(i) & 1, S.abort));
+            const bool got = __all_sync(0xffffffffu, wait_or_abort(v_ready + b, use_of(i) & 1, S.abort, P.wait_clocks) &&
+                                                         wait_or_abort(mma_done + b, use_of(i) & 1, S.abort, P.wait_clocks));
             tc_fence_after();
             const size_t gpos = (size_t)bt * npos + pos0;  // first coefficient of the tile in the partial buffers
             if (part.mode != CRT_FULL && part.add_s && hf == 0 && valid) {
@@ -827,14 +828,38 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     if (threadIdx.x == 0 && *S.abort) {
         flag_error(P.status, DEV_ERR_WAIT);
         // copies and MMAs still in flight must land before this CTA's memory goes away
-        if (!b_seen) mbar_wait_bounded(bar_b, 0);
-        if (issued) mbar_wait_bounded(mma_done + buf_of(issued - 1), use_of(issued - 1) & 1);
-        if (b_pend) mbar_wait_bounded(bar_b, b_par);
+        if (!b_seen) mbar_wait_bounded(bar_b, 0, P.wait_clocks);
+        if (issued) mbar_wait_bounded(mma_done + buf_of(issued - 1), use_of(issued - 1) & 1, P.wait_clocks);
+        if (b_pend) mbar_wait_bounded(bar_b, b_par, P.wait_clocks);
     }
     // the last prime block's ab_free arrival (its MMAs are complete: the epilogue waited for them)
-    if (threadIdx.x == 0 && ab_commits) mbar_wait_bounded(ab_free, (ab_commits - 1) & 1);
+    if (threadIdx.x == 0 && ab_commits) mbar_wait_bounded(ab_free, (ab_commits - 1) & 1, P.wait_clocks);
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, nbuf * AS);
+}
+
+// Self-test of the bounded waits (pm_selftest_wait): one block waits on an mbarrier that nothing
+// arrives on -- thread 0 with mbar_wait_bounded, warp 1 with wait_or_abort, whose first lane to
+// time out raises the shared abort flag for the others -- and must give up after `limit` clocks
+// with DEV_ERR_WAIT in *status.  Then thread 0 arrives, and every thread's wait on the
+// completed phase must succeed (bit 8 of *status if one does not).  No copy or MMA is in flight
+// at any point, so giving up leaves nothing behind.
+__global__ void __launch_bounds__(64) k_wait_selftest(uint32_t* status, long long limit) {
+    __shared__ uint64_t bar;
+    __shared__ int abort_f;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        abort_f = 0;
+    }
+    __syncthreads();
+    bool gave_up = false;
+    if (threadIdx.x == 0) gave_up = !mbar_wait_bounded(&bar, 0, limit);
+    else if (threadIdx.x >= 32) gave_up = !wait_or_abort(&bar, 0, &abort_f, limit);
+    if (gave_up) flag_error(status, DEV_ERR_WAIT);
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_arrive(&bar);
+    __syncthreads();
+    if (!mbar_wait_bounded(&bar, 0, limit + 1000000ll)) flag_error(status, 1u << 8);
 }
 
 size_t rns_tc_smem(const DevPlan& P, int ring) {
@@ -873,7 +898,7 @@ __global__ void __launch_bounds__(TC_M) k_crt_finish(DevPlan P, const uint32_t* 
         if (fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
         const uint32_t v = (uint32_t)min(max((int)vf, 0), 2 * P.K);  // residues unreduced: v < 2K
         uint32_t* z = zrow + (size_t)m * zs;
-        const uint32_t* T1 = P.tneg + L;
+        const uint32_t* T1 = P.t1;
         uint64_t carry = 0;
         for (int l = 0; l < zl; ++l) {
             const uint64_t t = (uint64_t)z[l] + carry + (l < L ? (uint64_t)v * __ldg(T1 + l) : 0ull);

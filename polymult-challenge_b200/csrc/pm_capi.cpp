@@ -1,5 +1,7 @@
 // pm_capi.cpp -- the extern "C" boundary (include/polymult_b200.h).  Exceptions never cross
 // it: each entry point maps them to a status code and keeps the message per thread.
+#include <cuda_runtime.h>
+
 #include <cstring>
 #include <new>
 #include <string>
@@ -7,6 +9,7 @@
 
 #include "../../include/polymult_b200.h"
 #include "pm_context.h"
+#include "pm_kernels.cuh"
 
 namespace pm {
 
@@ -23,6 +26,21 @@ using pm::fail;
 using pm::g_last_error;
 
 namespace {
+
+// Restores the caller's current device on scope exit: the entry points that run an engine
+// switch to the engine's device, which a framework calling them does not expect to change.
+struct DeviceScope {
+    int saved = -1;
+    DeviceScope() {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            saved = -1;
+            cudaGetLastError();
+        }
+    }
+    ~DeviceScope() {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
 
 template <class F>
 int guarded(F&& f) {
@@ -72,6 +90,7 @@ int pm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_form
 int pm_run(pm_context* ctx, const uint32_t* a, const uint32_t* b, uint32_t* c) {
     if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
     if (!a || !b || !c) return fail(PM_ERR_INVALID, "null operand");
+    DeviceScope keep;
     return guarded([&] { ctx->engine->run_host(a, b, c); });
 }
 
@@ -79,26 +98,53 @@ int pm_run_device(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uin
                   void* stream) {
     if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
     if (count && (!d_a || !d_b || !d_c)) return fail(PM_ERR_INVALID, "null operand");
+    DeviceScope keep;
     return guarded([&] { ctx->engine->run_device(d_a, d_b, d_c, count, static_cast<cudaStream_t>(stream)); });
+}
+
+int pm_run_device_static(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream) {
+    if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    if (!d_a || !d_b || !d_c) return fail(PM_ERR_INVALID, "null operand");
+    DeviceScope keep;
+    return guarded([&] { pm::run_device_static(*ctx->engine, d_a, d_b, d_c, static_cast<cudaStream_t>(stream)); });
 }
 
 int pm_time_stages(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, uint32_t count,
                    int reps, void* stream, float* ms_out) {
     if (!ctx || !ctx->engine || !ms_out) return fail(PM_ERR_INVALID, "null argument");
     if (!d_a || !d_b || !d_c) return fail(PM_ERR_INVALID, "null operand");
+    DeviceScope keep;
     return guarded(
         [&] { ctx->engine->time_stages(d_a, d_b, d_c, count, reps, static_cast<cudaStream_t>(stream), ms_out); });
 }
 
 int pm_sync(pm_context* ctx) {
     if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    DeviceScope keep;
     return guarded([&] { ctx->engine->throw_if_status(); });
 }
 
 void pm_free(pm_context* ctx) {
     if (!ctx) return;
+    DeviceScope keep;
+    if (ctx->engine) pm::forget_static_scratch_address(ctx->engine->device());
     delete ctx->engine;
     delete ctx;
+}
+
+void pm_test_fail_scratch_allocs(int skip, int n) { pm::inject_scratch_alloc_failures(skip, n); }
+
+int pm_test_set_status(pm_context* ctx, uint32_t bits) {
+    if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    DeviceScope keep;
+    return guarded([&] { ctx->engine->set_status_for_test(bits); });
+}
+
+int pm_selftest_wait(int device, uint64_t limit_clocks, uint32_t* status_out) {
+    if (!status_out || limit_clocks == 0 || limit_clocks > (uint64_t)pm::kWaitClocks)
+        return fail(PM_ERR_INVALID, "bad self-test arguments");
+    DeviceScope keep;
+    return guarded([&] { *status_out = pm::wait_selftest(device, (long long)limit_clocks); });
 }
 
 int pm_get_info(const pm_context* ctx, pm_info* out) {
@@ -243,7 +289,8 @@ const char* pm_last_error(void) { return g_last_error.c_str(); }
 
 int pm_selftest_host_pool(uint32_t pools, uint32_t runs, uint32_t workers, int vary, uint64_t* failures) {
     if (!failures || workers > 63) return fail(PM_ERR_INVALID, "bad self-test arguments");
-    return guarded([&] { *failures = pm::host_pool_selftest(pools, runs, (int)workers, vary != 0); });
+    return guarded(
+        [&] { *failures = pm::host_pool_selftest(pools, runs, (int)workers, (vary & 1) != 0, (vary & 2) != 0); });
 }
 
 int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int32_t* K_out) {

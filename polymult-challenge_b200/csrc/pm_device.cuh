@@ -17,7 +17,7 @@ namespace pm {
 // Device status word bits (read back by the host after a run).
 enum : uint32_t {
     DEV_ERR_CRT_BOUND = 1u,   // fp32 CRT estimate not within 1/4 of an integer (|x| < M/8 violated)
-    DEV_ERR_FOLD = 2u,        // delta-fold did not converge within its iteration bound
+    DEV_ERR_FOLD = 2u,        // the CRT value had bits above 2^W after its folds (outside its bound)
     DEV_ERR_WAIT = 4u,        // an mbarrier wait hit its iteration limit
 };
 
@@ -25,7 +25,9 @@ enum : uint32_t {
 struct DevPlan {
     uint32_t N, nrows, ncols;
     int logN, w1, w2;
-    int K, KP, L, W, HP;
+    int K, KP, L, W;
+    int D, DP;                // 24-bit digits of a W-bit value (DP: rounded up to a multiple of 4)
+    int fold_count;           // CRT folds z -> (z mod 2^W) + (z >> W) delta before the final -q
     int Kr;                   // primes of the residue arrays R[batch][Kr][N] (K except in a prime block)
     uint64_t delta;
     const uint32_t* p;        // [KP]
@@ -34,9 +36,9 @@ struct DevPlan {
     const uint32_t* crt_cc;   // [KP]
     const float* rcp;         // [KP]
     const uint2* tw;          // [K][N] {psi^bitrev(k), floor(psi^bitrev(k) 2^32 / p)} (Shoup form)
-    const uint32_t* dec16;    // [2L][KP]
-    const uint16_t* qh16;     // [KP][HP]
-    const uint32_t* tneg;     // [K+1][L]
+    const uint32_t* dec24;    // [DP][KP] 2^(24 d) R mod p_j
+    const uint32_t* crt24;    // [K+1][DP] 24-bit digits of Q_j = (M/p_j) mod q; row K: of T_1
+    const uint32_t* t1;       // [L] T_1 = (-M) mod q
     const uint32_t* q;        // [L]
     const uint8_t* dec_b;     // tensor-core decomposition B operand (canonical image)
     const uint8_t* dec_b_ra;  // the same, constants times gamma_j = crt_c_j 2^-32 (operand RA)
@@ -45,6 +47,7 @@ struct DevPlan {
     int dec_nrows, dec_kbytes;
     int crt_nrows, crt_kbytes;
     uint32_t* status;         // device status word
+    long long wait_clocks;    // limit of every mbarrier wait of the tcgen05 kernels (2e9 clocks, ~1 s)
 };
 
 // A chunk of coefficient positions: all rows x `cw` columns starting at `col0`, stored

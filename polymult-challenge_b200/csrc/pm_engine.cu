@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "pm_kernels.cuh"
 
@@ -34,111 +35,6 @@ void cuda_check(cudaError_t e, const char* what) {
 }
 
 void throw_cuda(cudaError_t e, const char* what) { throw CudaError(std::string(what) + ": " + cudaGetErrorString(e)); }
-
-// ---------------------------------------------------------------------------------------
-// host pool
-// ---------------------------------------------------------------------------------------
-HostPool::HostPool(int workers, int idle_us) : idle_us_(idle_us) {
-    for (int i = 0; i < workers; ++i) threads_.emplace_back([this] { loop(); });
-}
-
-HostPool::~HostPool() {
-    stop_.store(true);
-    {
-        std::lock_guard<std::mutex> lk(m_);
-        cv_.notify_all();
-    }
-    for (auto& t : threads_) t.join();
-}
-
-// Claims and runs one task of generation `gen`; false when there is none left to claim.
-bool HostPool::work_once(uint64_t gen) {
-    uint64_t c = claim_.load(std::memory_order_acquire);
-    for (;;) {
-        // unsigned: a closed generation's index (all ones) is past every task count
-        if ((c >> 32) != gen || (uint32_t)c >= (uint32_t)n_.load(std::memory_order_acquire)) return false;
-        if (claim_.compare_exchange_weak(c, c + 1, std::memory_order_acq_rel, std::memory_order_acquire)) break;
-    }
-    (*fn_)((int)(uint32_t)c);
-    done_.fetch_add(1, std::memory_order_acq_rel);
-    return true;
-}
-
-void HostPool::run(int n, const std::function<void(int)>& fn) {
-    if (n <= 0) return;
-    const uint64_t prev = claim_.load(std::memory_order_relaxed) >> 32, gen = prev + 1;
-    // Close the previous generation first: its claim word gets an index no task count reaches,
-    // so a worker that read it (or the count) before this run cannot claim a task under it --
-    // its compare-exchange fails on the changed word.  Only then the task, its count and the
-    // completion counter change; the new generation's word publishes them (release).
-    claim_.store((prev << 32) | 0xFFFFFFFFull, std::memory_order_seq_cst);
-    fn_ = &fn;
-    n_.store(n, std::memory_order_seq_cst);
-    done_.store(0, std::memory_order_seq_cst);
-    claim_.store(gen << 32, std::memory_order_release);
-    if (sleepers_.load() > 0) {
-        std::lock_guard<std::mutex> lk(m_);
-        cv_.notify_all();
-    }
-    while (work_once(gen)) {
-    }
-    while (done_.load(std::memory_order_acquire) < n) {
-#if defined(__x86_64__)
-        __builtin_ia32_pause();
-#endif
-    }
-}
-
-uint64_t host_pool_selftest(uint32_t pools, uint32_t runs, int workers, bool vary) {
-    uint64_t bad = 0;
-    std::vector<std::atomic<int>> hits(64);
-    for (uint32_t pi = 0; pi < pools; ++pi) {
-        HostPool pool(workers);  // as pm_run's: workers spin between task sets
-        for (uint32_t it = 0; it < runs; ++it) {
-            const int n = vary ? 1 + (int)((it * 37u + pi) % 64u) : 64;
-            for (auto& h : hits) h.store(0, std::memory_order_relaxed);
-            std::atomic<int> inflight{0};
-            const std::function<void(int)> fn = [&](int t) {
-                inflight.fetch_add(1);
-                if (t >= 0 && t < 64) hits[t].fetch_add(1);
-                inflight.fetch_sub(1);
-            };
-            pool.run(n, fn);
-            bool ok = inflight.load() == 0;
-            for (int t = 0; t < 64 && ok; ++t) ok = hits[t].load() == (t < n ? 1 : 0);
-            if (!ok) ++bad;
-        }
-    }
-    return bad;
-}
-
-void HostPool::loop() {
-    using clock = std::chrono::steady_clock;
-    auto last = clock::now();
-    uint32_t spins = 0;
-    while (!stop_.load(std::memory_order_relaxed)) {
-        const uint64_t gen = claim_.load(std::memory_order_acquire) >> 32;
-        if (work_once(gen)) {
-            last = clock::now();
-            continue;
-        }
-#if defined(__x86_64__)
-        __builtin_ia32_pause();
-#endif
-        if ((++spins & 1023u) == 0 && clock::now() - last > std::chrono::microseconds(idle_us_)) {
-            sleepers_.fetch_add(1);
-            {
-                std::unique_lock<std::mutex> lk(m_);
-                cv_.wait_for(lk, std::chrono::milliseconds(100), [&] {
-                    const uint64_t c = claim_.load();
-                    return stop_.load() || ((c >> 32) != gen && (uint32_t)c < (uint32_t)n_.load());
-                });
-            }
-            sleepers_.fetch_sub(1);
-            last = clock::now();
-        }
-    }
-}
 
 namespace {
 
@@ -356,7 +252,9 @@ void Engine::upload_tables() {
     d.KP = P.KP;
     d.L = (int)P.L;
     d.W = (int)P.W;
-    d.HP = P.HP;
+    d.D = P.D;
+    d.DP = P.DP;
+    d.fold_count = P.fold_count;
     d.delta = P.delta;
     size_t* tb = &table_bytes_;
     d.p = dev_upload(dev_allocs_, P.p, tb);
@@ -365,9 +263,9 @@ void Engine::upload_tables() {
     d.crt_cc = dev_upload(dev_allocs_, P.crt_cc, tb);
     d.rcp = dev_upload(dev_allocs_, P.rcp, tb);
     d.tw = reinterpret_cast<const uint2*>(dev_upload(dev_allocs_, P.tw, tb));
-    d.dec16 = dev_upload(dev_allocs_, P.dec16, tb);
-    d.qh16 = dev_upload(dev_allocs_, P.qh16, tb);
-    d.tneg = dev_upload(dev_allocs_, P.tneg, tb);
+    d.dec24 = dev_upload(dev_allocs_, P.dec24, tb);
+    d.crt24 = dev_upload(dev_allocs_, P.crt24, tb);
+    d.t1 = dev_upload(dev_allocs_, P.t1, tb);
     d.q = dev_upload(dev_allocs_, P.q, tb);
     d.dec_b = dev_upload(dev_allocs_, P.dec_b, tb);
     d.dec_b_ra = dev_upload(dev_allocs_, P.dec_b_ra, tb);
@@ -380,15 +278,39 @@ void Engine::upload_tables() {
     uint32_t* st = dev_alloc<uint32_t>(dev_allocs_, 1, nullptr);
     cuda_check(cudaMemset(st, 0, 4), "memset status");
     d.status = st;
+    d.wait_clocks = kWaitClocks;
+}
+
+void Engine::set_status_for_test(uint32_t bits) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    cuda_check(cudaDeviceSynchronize(), "device synchronize");
+    cuda_check(cudaMemcpy(dp_.status, &bits, 4, cudaMemcpyHostToDevice), "status write");
+}
+
+uint32_t wait_selftest(int device, long long limit) {
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    uint32_t* st = nullptr;
+    cuda_check(cudaMalloc(&st, 4), "cudaMalloc");
+    uint32_t out = 0;
+    cudaError_t e = cudaMemset(st, 0, 4);
+    if (e == cudaSuccess) e = launch_kernel(k_wait_selftest, dim3(1), dim3(64), 0, nullptr, false, st, limit);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&out, st, 4, cudaMemcpyDeviceToHost);
+    cudaFree(st);
+    if (e != cudaSuccess) throw_cuda(e, "wait self-test");
+    return out;
 }
 
 void Engine::setup_launch_shapes() {
     rpb_ = ntt_rows_per_cta(plan_.w2);
     smem_cols_ = ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(32, plan_.ncols)));
     if (smem_cols_ > smem_optin_) throw Unsupported("NTT tile exceeds shared memory");
-    dec_tab_smem_ = rns_plain_smem(dp_, true) <= 100 * 1024;
+    // the plain kernels stage their constant tables in shared memory while two blocks still fit
+    // an SM (up to W = 1747 or so); beyond that they read them through L1
+    dec_tab_smem_ = rns_plain_smem(dp_, true) <= 110 * 1024;
     smem_dec_ = rns_plain_smem(dp_, dec_tab_smem_);
-    smem_crt_ = crt_plain_smem(dp_);
+    crt_tab_smem_ = crt_plain_smem(dp_, true) <= 110 * 1024;
+    smem_crt_ = crt_plain_smem(dp_, crt_tab_smem_);
     if (smem_dec_ > smem_optin_ || smem_crt_ > smem_optin_) throw Unsupported("plain GEMM tile exceeds shared memory");
     // Every kernel may use up to the device's opt-in maximum: contexts for different points
     // share these kernels, so a per-point limit set by one context could fail another's launch.
@@ -414,14 +336,46 @@ void Engine::setup_launch_shapes() {
     cuda_check(cudaFuncSetAttribute(k_crt_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
 }
 
+// Test hook (pm_test_fail_scratch_allocs): after `skip` more residue-scratch allocations, the
+// next `n` fail on the host as if cudaMalloc had run out of memory.
+static std::mutex g_inject_mutex;
+static int g_inject_skip = 0, g_inject_fail = 0;
+void inject_scratch_alloc_failures(int skip, int n) {
+    std::lock_guard<std::mutex> lk(g_inject_mutex);
+    g_inject_skip = std::max(0, skip);
+    g_inject_fail = std::max(0, n);
+}
+
+static cudaError_t scratch_malloc(void** p, size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(g_inject_mutex);
+        if (g_inject_skip > 0) --g_inject_skip;
+        else if (g_inject_fail > 0) {
+            --g_inject_fail;
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
 void Engine::ensure_scratch(uint32_t group) {
     if (group <= group_) return;
+    // the engine holds no scratch from here until both arrays exist: a failed allocation leaves
+    // group_ = 0, so the next call allocates again instead of launching on missing arrays
     if (d_ra_) cudaFree(d_ra_);
     if (d_rb_) cudaFree(d_rb_);
     d_ra_ = d_rb_ = nullptr;
+    group_ = 0;
+    scratch_words_ = 0;
     const size_t words = (size_t)group * plan_.K * plan_.N;
-    cuda_check(cudaMalloc(&d_ra_, words * 4), "cudaMalloc residues");
-    cuda_check(cudaMalloc(&d_rb_, words * 4), "cudaMalloc residues");
+    cuda_check(scratch_malloc(reinterpret_cast<void**>(&d_ra_), words * 4), "cudaMalloc residues");
+    const cudaError_t e = scratch_malloc(reinterpret_cast<void**>(&d_rb_), words * 4);
+    if (e != cudaSuccess) {
+        cudaFree(d_ra_);
+        d_ra_ = nullptr;
+        throw_cuda(e, "cudaMalloc residues");
+    }
     scratch_words_ = 2 * words;
     group_ = group;
 }
@@ -881,7 +835,8 @@ void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out,
                    "launch k_crt_finish");
     } else {
         dim3 grid((npos + CRT_TM - 1) / CRT_TM, 1, nb);
-        cuda_check(launch_kernel(k_crt_plain, grid, dim3(128), smem_crt_, s, pdl, dp_, R, chunk_map(ch), npos, out),
+        cuda_check(launch_kernel(k_crt_plain, grid, dim3(256), smem_crt_, s, pdl, dp_, R, chunk_map(ch), npos, out,
+                                 crt_tab_smem_ ? 1 : 0),
                    "launch k_crt_plain");
     }
 }
@@ -995,7 +950,7 @@ void Engine::throw_if_status() {
     if (st) {
         std::string what = "device-side check failed:";
         if (st & DEV_ERR_CRT_BOUND) what += " CRT estimate outside its exactness bound;";
-        if (st & DEV_ERR_FOLD) what += " delta-fold did not converge;";
+        if (st & DEV_ERR_FOLD) what += " CRT value outside its bound after folding;";
         if (st & DEV_ERR_WAIT) what += " tensor-core wait timed out;";
         throw DeviceCheckError(what);
     }
@@ -1188,7 +1143,7 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         *h_status_ = 0;
         std::string what = "device-side check failed:";
         if (st & DEV_ERR_CRT_BOUND) what += " CRT estimate outside its exactness bound;";
-        if (st & DEV_ERR_FOLD) what += " delta-fold did not converge;";
+        if (st & DEV_ERR_FOLD) what += " CRT value outside its bound after folding;";
         if (st & DEV_ERR_WAIT) what += " tensor-core wait timed out;";
         throw DeviceCheckError(what);
     }

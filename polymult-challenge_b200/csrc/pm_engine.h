@@ -6,17 +6,16 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
-#include <condition_variable>
 #include <cstdint>
 #include <functional>
 #include <memory>
-#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "pm_device.cuh"
+#include "pm_hostpool.h"
 #include "pm_plan.h"
 
 namespace pm {
@@ -32,39 +31,18 @@ struct Unsupported : std::runtime_error {
 };
 
 void cuda_check(cudaError_t e, const char* what);
+// Test hook: after `skip` more residue-scratch allocations of any engine, the next `n` fail
+// (host-side injection).
+void inject_scratch_alloc_failures(int skip, int n);
 
-// Host worker pool for the pageable <-> pinned staging copies.  run(n, fn) executes
-// fn(0..n-1) across the workers and the calling thread and returns when all are done.
-// Workers spin between jobs (a job every few tens of microseconds is the pipeline's rhythm;
-// a condition-variable wake-up per job would cost more than the copy) and fall back to
-// sleeping after `idle_us` without work.  Task indices are claimed with a compare-and-swap
-// on (generation << 32 | next index), so a worker still finishing an old job can never take
-// a task of the next one.
-// Stress test of HostPool::run (pm_selftest_host_pool): task sets whose tasks did not each run
-// exactly once, or were still running when run() returned.
-uint64_t host_pool_selftest(uint32_t pools, uint32_t runs, int workers, bool vary);
-
-class HostPool {
-  public:
-    explicit HostPool(int workers, int idle_us = 200000);
-    ~HostPool();
-    void run(int n, const std::function<void(int)>& fn);
-    int size() const { return (int)threads_.size() + 1; }
-
-  private:
-    void loop();
-    bool work_once(uint64_t gen);
-    std::vector<std::thread> threads_;
-    std::atomic<uint64_t> claim_{0};     // (generation << 32) | next task index
-    std::atomic<int> done_{0};
-    std::atomic<int> n_{0};
-    std::atomic<bool> stop_{false};
-    std::atomic<int> sleepers_{0};
-    const std::function<void(int)>* fn_ = nullptr;
-    int idle_us_;
-    std::mutex m_;
-    std::condition_variable cv_;
-};
+class Engine;
+// pm_run_device_static's body (pm_static_scratch.cu): one multiply with the library's static
+// residue scratch; throws InvalidPoint for a point beyond it.
+void run_device_static(Engine& e, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t stream);
+// drops the cached device address of the static scratch on `device` (pm_free)
+void forget_static_scratch_address(int device);
+// runs k_wait_selftest on `device` with a wait limit of `limit` clocks; returns its status word
+uint32_t wait_selftest(int device, long long limit);
 
 enum GemmForm : int { GEMM_AUTO = 0, GEMM_PLAIN = 1, GEMM_TENSOR = 2, GEMM_MIXED = 3 };
 
@@ -116,6 +94,9 @@ class Engine {
     // Reads (and clears) the device status word; synchronises with the device.
     uint32_t take_status();
     void throw_if_status();
+    // Test hook: writes `bits` into the device status word (after the device is idle), as a
+    // failed device-side check would.
+    void set_status_for_test(uint32_t bits);
 
     const Plan& plan() const { return plan_; }
     const DevPlan& dev() const { return dp_; }
@@ -210,7 +191,7 @@ class Engine {
     int rpb_ = 1;
     size_t smem_cols_ = 0;
     size_t smem_dec_ = 0, smem_crt_ = 0;
-    bool dec_tab_smem_ = false;
+    bool dec_tab_smem_ = false, crt_tab_smem_ = false;
 
     // host pipeline
     std::vector<Chunk> cin_[2], cout_[2];

@@ -52,12 +52,13 @@ void ntt_probe_images(int w1, int w2);              // throws CudaError if an im
 size_t ntt_cols_smem(const DevPlan& P, int ltc);
 
 // ---- plain (CUDA-core) RNS decomposition and CRT (k_rns.cu)
-constexpr int DEC_TM = 64;   // coefficients per decomposition block
-constexpr int CRT_TM = 32;   // coefficients per CRT block
+constexpr int DEC_TM = 64;   // coefficients per decomposition block (256 threads)
+constexpr int CRT_TM = 64;   // coefficients per CRT block (256 threads)
+// tab_in_smem: the block stages its constant table (digits x primes) in shared memory
 __global__ void k_rns_plain(DevPlan P, const uint32_t* src, ChunkMap C, uint32_t npos, uint32_t* R, int tab_in_smem);
-__global__ void k_crt_plain(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t* out);
+__global__ void k_crt_plain(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t* out, int tab_in_smem);
 size_t rns_plain_smem(const DevPlan& P, bool tab_in_smem);
-size_t crt_plain_smem(const DevPlan& P);
+size_t crt_plain_smem(const DevPlan& P, bool tab_in_smem);
 
 // ---- tensor-core (tcgen05 kind::i8) RNS decomposition and CRT (k_tc.cu)
 constexpr int TC_M = 128;    // coefficients per UMMA tile (TMEM lanes)
@@ -78,6 +79,9 @@ struct CrtPartial {
 __global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
                          CrtPartial part, CrtPrimeBlocks pbs);
 __global__ void k_crt_finish(DevPlan P, const uint32_t* zp, const float* sp, uint32_t total, uint32_t* out);
+// the bounded waits made to run out (pm_selftest_wait): 64 threads, one block
+__global__ void k_wait_selftest(uint32_t* status, long long limit);
+constexpr long long kWaitClocks = 2000000000ll;  // DevPlan::wait_clocks
 constexpr int RNS_TC_THREADS = 640;  // 4 loader warps + 16 epilogue warps (4 lane quarters x 2 prime halves x 2 column sets)
 constexpr int CRT_TC_THREADS = 512;  // 256 producers + 256 epilogue threads, two per coefficient each
 size_t rns_tc_smem(const DevPlan& P, int ring = 2);

@@ -1,12 +1,18 @@
 // pm_plan.h -- host-side precompute for one (N, W, q) point: RNS primes, twiddle tables,
-// decomposition and CRT constants, and the byte-sliced operand tables of the tensor-core
-// GEMMs.  Pure C++ (no CUDA), so the host logic is testable on a machine without a GPU.
+// the constants of the plain (CUDA-core) GEMMs, the byte-sliced operand images of the
+// tensor-core GEMMs, and the bound that fixes the CRT's fold count.  Pure C++ (no CUDA), so
+// the host logic is testable on a machine without a GPU.
 //
-// Replaces the reference's precompute() (solve.cu:869-1020) with a different prime family:
-// primes p < 2^30 with p == 1 (mod 2*max(N, 2^16)).  Below 2^30, 4p < 2^32, so every NTT
-// stage can keep its values lazily in [0, 4p) (Harvey butterflies) instead of reducing to
-// [0, p) after each butterfly; and one prime list serves every N <= 2^16, which the batched
-// path relies on.
+// Replaces the reference's precompute() (solve.cu:869-1020) with a different design:
+//   * primes p < 2^30 with p == 1 (mod 2 max(N, 2^16)), found by trial division against a
+//     sieve of the primes below 2^15: below 2^30, 4p < 2^32, so every NTT stage keeps its values
+//     lazily in [0, 4p) (Harvey butterflies), and one prime list serves every N <= 2^16, which
+//     the batched path relies on;
+//   * psi from a quadratic non-residue (the 2-power part of the multiplicative group,
+//     Tonelli-Shanks style) instead of a search over candidate generators;
+//   * M / p_j by exact division of the bigint M, which gives both (M / p_j) mod p_j and
+//     Q_j = (M / p_j) mod q;
+//   * the plain GEMMs work on 24-bit digits (the reference's on 16-bit halves).
 #pragma once
 
 #include <cstddef>
@@ -32,14 +38,17 @@ struct GemmShape {
     size_t b_bytes() const { return (size_t)n_rows * k_bytes; }
 };
 
+// Bits per digit of the plain GEMMs.  A 30-bit factor times a 24-bit digit is below 2^54, so
+// up to 1023 such products sum exactly in 64 bits.
+constexpr int kDigitBits = 24;
+
 struct Plan {
     // point
     uint32_t N = 0, W = 0, L = 0;
     int logN = 0, w1 = 0, w2 = 0;     // 4-step split: nrows = 2^w1 (column pass), ncols = 2^w2
     uint32_t nrows = 1, ncols = 1;
     std::vector<uint32_t> q;          // [L]
-    uint64_t delta = 0;               // 2^W - q
-    int delta_bits = 0;
+    uint64_t delta = 0;               // 2^W - q (< 2^63)
 
     // RNS
     int K = 0;                        // primes
@@ -55,11 +64,18 @@ struct Plan {
     // k < N (two words per entry)
     std::vector<uint32_t> tw;         // [K][N][2]
 
-    // plain (CUDA-core) GEMM tables
-    int HP = 0;                       // 2L rounded up to a multiple of 4
-    std::vector<uint32_t> dec16;      // [2L][KP]  2^(16h) R mod p_j
-    std::vector<uint16_t> qh16;       // [KP][HP]  16-bit halves of Q_j = (M/p_j) mod q
-    std::vector<uint32_t> tneg;       // [K+1][L]  (-v M) mod q
+    // plain (CUDA-core) GEMM tables, 24-bit digits: a coefficient is sum_d digit_d 2^(24 d)
+    int D = 0;                        // digits of a W-bit value: ceil(W / 24)
+    int DP = 0;                       // D rounded up to a multiple of 4
+    std::vector<uint32_t> dec24;      // [DP][KP]  2^(24 d) R mod p_j (0 for d >= D)
+    std::vector<uint32_t> crt24;      // [K + 1][DP] 24-bit digits of Q_j = (M/p_j) mod q; row K: of T_1
+    std::vector<uint32_t> t1;         // [L]  T_1 = (-M) mod q
+
+    // The CRT's value before reduction is below crt_bound (sum over primes of y'_j Q_j with
+    // y'_j < 2 p_j, plus v' T_1 with v' < 2K); fold_count folds z -> (z mod 2^W) + (z >> W) delta
+    // bring every such value below 2q, after which one conditional subtraction of q finishes.
+    std::vector<uint32_t> crt_bound;  // bigint limbs
+    int fold_count = 1;
 
     // tensor-core GEMM tables (canonical smem images, uploaded as-is)
     GemmShape dec_gemm;               // rows (j,t) = 4j+t, K = coefficient bytes

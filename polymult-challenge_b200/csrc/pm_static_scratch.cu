@@ -1,6 +1,6 @@
-// pm_static_scratch.cu -- pm_run_device_static: the device-resident multiply with its residue
-// scratch in a fixed device array compiled into this library, so that the call allocates
-// nothing.
+// pm_static_scratch.cu -- the scratch of pm_run_device_static: the device-resident multiply
+// with its residue scratch in a fixed device array compiled into this library, so that the
+// call allocates nothing.
 //
 // Who needs it: callers that cannot call cudaMalloc while they compute.  Examples are a host
 // framework that owns the device memory through its own caching allocator (it has reserved the
@@ -21,68 +21,59 @@
 // In host code `g_residue_scratch` names a host-side stand-in, not device memory, so it is never
 // passed to a kernel.  The device address is looked up once per device, with that device
 // current, by cudaGetSymbolAddress, on the first call on that device; make that first call
-// before any stream capture.
+// before any stream capture.  pm_free forgets the looked-up address of its context's device,
+// so the next call looks it up again (after a cudaDeviceReset the old address is stale: free
+// every context of a device before resetting it).
 #include <cstdint>
 #include <mutex>
 #include <string>
 
-#include "../../include/polymult_b200.h"
-#include "pm_context.h"
-
-namespace pm {
-int fail(int code, const char* what);
-extern thread_local std::string g_last_error;
-}  // namespace pm
-
-namespace {
+#include "pm_engine.h"
+#include "pm_kernels.cuh"
 
 constexpr size_t kStaticScratchWords = size_t(16) << 20;  // 64 MiB
-__device__ __align__(256) uint32_t g_residue_scratch[kStaticScratchWords];
+static __device__ __align__(256) uint32_t g_residue_scratch[kStaticScratchWords];
+
+namespace pm {
+namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_lookup_mutex;
 uint32_t* g_device_address[kMaxDevices] = {};
 
 // Device address of g_residue_scratch on `device` (which must be current).
-cudaError_t scratch_address(int device, uint32_t** out) {
+uint32_t* scratch_address(int device) {
     std::lock_guard<std::mutex> lk(g_lookup_mutex);
     if (!g_device_address[device]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_residue_scratch);
-        if (e != cudaSuccess) return e;
+        if (e != cudaSuccess) throw_cuda(e, "cudaGetSymbolAddress of the static scratch");
         g_device_address[device] = static_cast<uint32_t*>(p);
     }
-    *out = g_device_address[device];
-    return cudaSuccess;
+    return g_device_address[device];
 }
 
 }  // namespace
 
-extern "C" int pm_run_device_static(pm_context* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
-                                    void* stream) {
-    if (!ctx || !ctx->engine) return pm::fail(PM_ERR_INVALID, "null context");
-    if (!d_a || !d_b || !d_c) return pm::fail(PM_ERR_INVALID, "null operand");
-    pm::Engine& e = *ctx->engine;
+// The body of pm_run_device_static (pm_capi.cpp maps its exceptions to status codes and
+// restores the caller's current device).
+void run_device_static(Engine& e, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t stream) {
     const size_t words = (size_t)e.plan().K * e.plan().N;
-    if (2 * words > kStaticScratchWords) {
-        return pm::fail(PM_ERR_INVALID,
-                        ("pm_run_device_static: K*N = " + std::to_string(words) + " residue words per operand exceeds the " +
-                         std::to_string(kStaticScratchWords / 2) + " of the static scratch; use pm_run_device")
-                            .c_str());
-    }
+    if (2 * words > kStaticScratchWords)
+        throw InvalidPoint("pm_run_device_static: K*N = " + std::to_string(words) +
+                           " residue words per operand exceeds the " + std::to_string(kStaticScratchWords / 2) +
+                           " of the static scratch; use pm_run_device");
     const int dev = e.device();
-    if (dev < 0 || dev >= kMaxDevices) return pm::fail(PM_ERR_INVALID, "device index out of range");
-    cudaError_t ce = cudaSetDevice(dev);
-    if (ce != cudaSuccess) return pm::fail(PM_ERR_CUDA, cudaGetErrorString(ce));
-    uint32_t* ra = nullptr;
-    ce = scratch_address(dev, &ra);
-    if (ce != cudaSuccess)
-        return pm::fail(PM_ERR_CUDA, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce)).c_str());
-    try {
-        e.run_device_with_scratch(d_a, d_b, d_c, ra, ra + words, static_cast<cudaStream_t>(stream));
-    } catch (const std::exception& ex) {
-        return pm::fail(PM_ERR_CUDA, ex.what());
-    }
-    pm::g_last_error.clear();
-    return PM_OK;
+    if (dev < 0 || dev >= kMaxDevices) throw InvalidPoint("device index out of range");
+    cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+    uint32_t* ra = scratch_address(dev);
+    e.run_device_with_scratch(d_a, d_b, d_c, ra, ra + words, stream);
 }
+
+void forget_static_scratch_address(int device) {
+    if (device < 0 || device >= kMaxDevices) return;
+    std::lock_guard<std::mutex> lk(g_lookup_mutex);
+    g_device_address[device] = nullptr;
+}
+
+}  // namespace pm

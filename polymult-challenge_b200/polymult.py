@@ -27,6 +27,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libpolymult_b200.so")
 HEADER = os.path.join(HERE, "..", "include", "polymult_b200.h")
 
 PM_OK, PM_ERR_INVALID, PM_ERR_CUDA, PM_ERR_DEVICE, PM_ERR_UNSUPPORTED, PM_ERR_INTERNAL = range(6)
+PM_DEVICE_CRT_BOUND, PM_DEVICE_FOLD, PM_DEVICE_WAIT = 1, 2, 4  # device status word bits
 GEMM_FORMS = {"auto": 0, "plain": 1, "tensor": 2, "mixed": 3}
 GEMM_NAMES = {v: k for k, v in GEMM_FORMS.items()}
 STAGES = ("dec_a", "cols_a", "rows_a", "dec_b", "cols_b", "rows_fused", "cols_inv", "crt")
@@ -152,6 +153,12 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_server_host_free.restype = ctypes.c_int
     lib.pm_server_free.argtypes = [vp]
     lib.pm_server_free.restype = None
+    lib.pm_test_fail_scratch_allocs.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.pm_test_fail_scratch_allocs.restype = None
+    lib.pm_test_set_status.argtypes = [vp, ctypes.c_uint32]
+    lib.pm_test_set_status.restype = ctypes.c_int
+    lib.pm_selftest_wait.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]
+    lib.pm_selftest_wait.restype = ctypes.c_int
     del u32p
     _lib = lib
     return lib
@@ -169,11 +176,20 @@ def _u32(arr, shape=None) -> np.ndarray:
     return a
 
 
-def host_pool_selftest(pools: int, runs: int, workers: int = 7, vary: bool = False) -> int:
+def host_pool_selftest(pools: int, runs: int, workers: int = 7, vary: bool = False, park: bool = False) -> int:
     """Stress test of the host staging pool (pm_selftest_host_pool); returns the failures."""
     f = ctypes.c_uint64()
-    _check(load().pm_selftest_host_pool(pools, runs, workers, 1 if vary else 0, ctypes.byref(f)))
+    flags = (1 if vary else 0) | (2 if park else 0)
+    _check(load().pm_selftest_host_pool(pools, runs, workers, flags, ctypes.byref(f)))
     return f.value
+
+
+def wait_selftest(limit_clocks: int, device: int = 0) -> int:
+    """The tensor-core kernels' bounded mbarrier waits made to run out (pm_selftest_wait);
+    returns the kernel's status word (PM_DEVICE_WAIT expected, bit 8 never)."""
+    st = ctypes.c_uint32(0)
+    _check(load().pm_selftest_wait(device, limit_clocks, ctypes.byref(st)))
+    return st.value
 
 
 def plan_selfcheck(N: int, W: int, q_limbs) -> int:

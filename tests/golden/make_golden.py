@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Generates the golden fixtures in this directory from the reference's OWN checker.
 
-Run in a container that has the reference checked out (default /root/reference; override
-with POLYMULT_REFERENCE).  It imports the reference's tests/oracle.py unchanged and uses
+Run where the reference is checked out: by default a directory named `reference` beside
+this repository; POLYMULT_REFERENCE names another.  It imports the reference's tests/oracle.py unchanged and uses
 its spec-prime search, case generator and bigint negacyclic NTT to produce, per point:
 
   * q (hex) and delta = 2^W - q;
@@ -29,7 +29,8 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("POLYMULT_REFERENCE", "/root/reference")
+REF = os.environ.get("POLYMULT_REFERENCE",
+                     os.path.normpath(os.path.join(HERE, "..", "..", "..", "reference")))
 
 # (N, W, cases, mode) — tests/run_emu.sh:20-33, then the benchmark configurations.
 POINTS = [

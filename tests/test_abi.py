@@ -64,14 +64,17 @@ def test_invalid_points_rejected():
     rc, msg = _init_error(63, 256, 8, q256)
     assert rc == polymult.PM_ERR_INVALID and "power of two" in msg
     rc, msg = _init_error(64, 256, 7, q256[:7])
-    assert rc == polymult.PM_ERR_INVALID and "W / L" in msg
+    assert rc == polymult.PM_ERR_INVALID and "ceil(W / 32)" in msg
     even = list(q256)
     even[0] &= ~1
     rc, msg = _init_error(64, 256, 8, even)
-    assert rc == polymult.PM_ERR_INVALID and "q out of range" in msg
+    assert rc == polymult.PM_ERR_INVALID and "q is even" in msg
     small = [12345, 0, 0, 0, 0, 0, 0, 0]   # delta = 2^256 - q far above 2^63
     rc, msg = _init_error(64, 256, 8, small)
-    assert rc == polymult.PM_ERR_INVALID
+    assert rc == polymult.PM_ERR_INVALID and "too far below 2^W" in msg
+    big = [0xFFFFFFFF] * 8                 # 2^256 - 1 is not below 2^W... for W = 255
+    rc, msg = _init_error(64, 255, 8, big)
+    assert rc == polymult.PM_ERR_INVALID and "not below 2^W" in msg
     rc, msg = _init_error(1 << 21, 256, 8, q256)
     assert rc == polymult.PM_ERR_INVALID
 

@@ -1,12 +1,11 @@
 """The host thread pool that stages pm_run's pageable operands, stressed on the CPU (no GPU).
 
 A task set handed to the pool must run every task exactly once and have none still running
-when the call returns: the tasks capture the caller's stack.  An earlier pool published a new
-set's task count before closing the previous set's claim word, so a worker could claim a task
-under the old set -- running it with a stale task pointer, or counting it into the new set so
-that the call returned early; it crashed a pool's first call about once in a few thousand.
-Both shapes are exercised: many fresh pools (a first call each) and long runs of task sets of
-varying size."""
+when the call returns: the tasks capture the caller's stack.  The pool hands out tasks as
+tickets of one packed word (job, count, next ticket) with fetch_add, and replaces the job's
+function only after every task of the job has finished.  Three shapes are exercised: many fresh
+pools (a first call each), long runs of task sets of varying size, and task sets that find the
+workers parked on their futex and must wake them."""
 import pytest
 
 from conftest import ensure_library
@@ -22,6 +21,12 @@ def test_varying_task_counts():
     import polymult
     ensure_library()
     assert polymult.host_pool_selftest(pools=40, runs=1000, vary=True) == 0
+
+
+def test_parked_workers_are_woken():
+    import polymult
+    ensure_library()
+    assert polymult.host_pool_selftest(pools=4, runs=300, vary=True, park=True) == 0
 
 
 def test_argument_check():
