@@ -191,8 +191,12 @@ typedef struct pm_serve_stats {
 int pm_server_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const uint32_t* resident, uint32_t nresident,
                    uint64_t hbm_budget, uint32_t max_batch, uint32_t streams, int gemm_form, int device,
                    pm_server** out);
+/* digest: NULL, or n entries; digest[i] receives pm_digest of request i's result, computed on the
+ * device from the result itself before its copy to c[i] (so a long stream can reuse its host
+ * result buffers and still have every result checked). */
 int pm_server_run(pm_server* server, uint32_t n, const double* t_arrive, const uint32_t* sel,
-                  const uint32_t* const* a, uint32_t* const* c, double* latency, pm_serve_stats* stats);
+                  const uint32_t* const* a, uint32_t* const* c, double* latency, pm_serve_stats* stats,
+                  uint64_t* digest);
 /* Pinned host memory owned by the server (freed by pm_server_free if not before). */
 int pm_server_host_alloc(pm_server* server, size_t bytes, void** out);
 int pm_server_host_free(pm_server* server, void* p);
@@ -252,6 +256,14 @@ int pm_selftest_host_pool(uint32_t pools, uint32_t runs, uint32_t workers, int v
  * a later call allocates it again.  Lets tests drive the allocation-failure path without
  * exhausting a shared GPU.  (0, 0) switches the injection off. */
 void pm_test_fail_scratch_allocs(int skip, int n);
+
+/* No reference counterpart: 64-bit digests of `count` arrays of `words` u32 words each, lying
+ * contiguously in device memory (results of pm_run_device, for instance), into out[count] (host
+ * memory).  D(x) = sum over i of mix(i << 32 | x_i) mod 2^64, mix the splitmix64 finalizer; equal
+ * arrays give equal digests, and pm_digest_host computes the same value for host memory.
+ * Synchronous on `stream`. */
+int pm_digest(const uint32_t* d_words, uint64_t words, uint32_t count, void* stream, uint64_t* out);
+uint64_t pm_digest_host(const uint32_t* words, uint64_t n);
 
 /* Test hook: writes `bits` (PM_DEVICE_* below) into the context's device status word, as a
  * failed device-side check would; the next pm_sync or pm_run then reports PM_ERR_DEVICE and

@@ -54,7 +54,7 @@ __device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const StwF& st
             const Tw2 wm = w[m];
 #pragma unroll
             for (int i = 0; i < h; ++i) {
-                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p, m * h + i);
             }
         }
     }
@@ -74,8 +74,8 @@ __device__ __forceinline__ void radix_fwd2(uint32_t (&v)[1 << RB], uint32_t (&u)
             const Tw2 wm = w[m];
 #pragma unroll
             for (int i = 0; i < h; ++i) {
-                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
-                bfly_ct_sh(u[m * 2 * h + i], u[m * 2 * h + i + h], wm, p);
+                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p, 0);
+                bfly_ct_sh(u[m * 2 * h + i], u[m * 2 * h + i + h], wm, p, 1);
             }
         }
     }
@@ -94,6 +94,26 @@ __device__ __forceinline__ void radix_inv(uint32_t (&v)[1 << RB], const StwF& st
 #pragma unroll
             for (int i = 0; i < h; ++i) {
                 bfly_gs_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+            }
+        }
+    }
+}
+
+// The inverse network on two lines that share their twiddles.
+template <int RB, int T0, class StwF>
+__device__ __forceinline__ void radix_inv2(uint32_t (&v)[1 << RB], uint32_t (&u)[1 << RB], const StwF& stw,
+                                           uint32_t p) {
+#pragma unroll
+    for (int t = RB - 1; t >= T0; --t) {
+        const int h = (1 << RB) >> (t + 1);
+        const auto w = stw(t);
+#pragma unroll
+        for (int m = 0; m < (1 << t); ++m) {
+            const Tw2 wm = w[m];
+#pragma unroll
+            for (int i = 0; i < h; ++i) {
+                bfly_gs_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                bfly_gs_sh(u[m * 2 * h + i], u[m * 2 * h + i + h], wm, p);
             }
         }
     }
@@ -140,13 +160,28 @@ struct SmemRun {
 // so that every exchange of the phase layouts below is free of bank conflicts -- with
 // 16-byte vector access in the last phase for NB = 6, 7, 8.
 // ---------------------------------------------------------------------------------------
+#ifndef POLYMULT_ROW_LAYOUT
+#define POLYMULT_ROW_LAYOUT 0
+#endif
 template <int NB>
 struct RowCfg : LineCfg<NB> {
     using B = LineCfg<NB>;
     static constexpr int LPR = 1 << (NB - B::RB);
     static constexpr int GRP = LPR > 32 ? LPR : 32;
+    static constexpr int RPG = GRP / LPR;             // rows per shared-memory region
     static constexpr int ROWS_PER_CTA = 128 / LPR;   // 128 threads per CTA
     static constexpr bool VEC = NB >= 6 && NB <= 8;   // swizzle keeps runs of 4 contiguous
+    // Additive layout (NB = 7, 8): element x of region row rho at rho * RS + x + 4 (x >> 4) -- each
+    // 16-element segment padded to 20 words, the row stride RS chosen so that the rows of a warp
+    // start 32 / RPG banks apart.  Every access of a phase is then the thread's base plus a
+    // compile-time offset (an immediate in the instruction, no address arithmetic), and both
+    // exchanges are conflict-free: a scalar phase's 32 lanes cover 32 consecutive banks (row
+    // offsets 16 (NB = 8) or 8 (NB = 7) apart, lanes of a row consecutive), and a vector phase's
+    // quarter-warps (one row's 8 segments) start at 20 r mod 32 = {0, 20, 8, 28, 16, 4, 24, 12}.
+    static constexpr bool ADD = POLYMULT_ROW_LAYOUT && (NB == 7 || NB == 8);
+    static constexpr int RS = NB == 8 ? 336 : 168;
+    static constexpr int REGION = ADD ? RPG * RS : GRP * B::E;  // words per region
+    __host__ __device__ static constexpr int pos(int rho, int x) { return rho * RS + x + 4 * (x >> 4); }
     __host__ __device__ static constexpr uint32_t g(int i) {
         // G(input bit i of X >> 5) for each NB; NB <= 4 has a single phase and no exchange
         return NB == 5 || NB == 9 ? (i == 0 ? 2u : i == 1 ? 4u : i == 2 ? 8u : i == 3 ? 17u : 0u)
@@ -183,6 +218,33 @@ template <int NB, int K, bool TO_SMEM>
 __device__ __forceinline__ void row_xchg(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r) {
     using C = RowCfg<NB>;
     constexpr int b0 = C::b0(K);
+    if constexpr (C::ADD) {
+        // x(e) = x(0) + (e << b0) with disjoint bits, and x >> 4 splits the same way, so
+        // pos(rho, x(e)) = pos(rho, x(0)) + pos(0, e << b0) (for b0 = 0, e stays inside x(0)'s segment)
+        uint32_t* base = region + C::pos(rho, row_x<NB, K>(r, 0));
+        if constexpr (b0 == 0) {
+#pragma unroll
+            for (int q = 0; q < C::E / 4; ++q) {
+                uint4* a = reinterpret_cast<uint4*>(base + 4 * q);
+                if (TO_SMEM) *a = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                else {
+                    const uint4 u = *a;
+                    v[4 * q] = u.x;
+                    v[4 * q + 1] = u.y;
+                    v[4 * q + 2] = u.z;
+                    v[4 * q + 3] = u.w;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < C::E; ++e) {
+                uint32_t* a = base + C::pos(0, e << b0);
+                if (TO_SMEM) *a = v[e];
+                else v[e] = *a;
+            }
+        }
+        return;
+    }
     // the register bits of X are zero in the base: X(e) = base ^ (e << b0)
     const int sbase = C::swz((rho << NB) | row_x<NB, K>(r, 0));
     if constexpr (C::VEC && b0 == 0) {
@@ -345,12 +407,12 @@ __global__ void __launch_bounds__(128, rows_min_blocks(NB, MODE)) k_ntt_rows(Dev
                                                                            const uint32_t* __restrict__ RA,
                                                                            const uint32_t* __restrict__ ra_sel) {
     using C = RowCfg<NB>;
-    constexpr int REGION_WORDS = C::NPH > 1 ? 128 * C::E : 4;
+    constexpr int REGION_WORDS = C::NPH > 1 ? (128 / C::GRP) * C::REGION : 4;  // one operand's regions
     __shared__ __align__(16) uint32_t sh[MODE == ROWS_BOTH ? 2 * REGION_WORDS : REGION_WORDS];
     const int tid = threadIdx.x;
     const int li = tid % C::GRP;                 // thread within the shared-memory region
     const int rho = li / C::LPR, r = li % C::LPR;
-    uint32_t* region = sh + (tid / C::GRP) * (C::GRP * C::E);
+    uint32_t* region = sh + (tid / C::GRP) * C::REGION;
     // the grid is (row blocks, primes, batch); blocks take them batch entry fastest in launch
     // order, so the nb blocks of one (row block, prime), which read the same twiddles, run
     // side by side and share them in L2
@@ -467,6 +529,93 @@ __device__ __forceinline__ void col_phases(uint32_t* tile, const Tw2* tws, uint3
 
 }  // namespace
 
+// Two-column form (lines of 2^NB >= 128 rows, tiles of 64 columns): thread t owns columns
+// 2 (t % 32) and 2 (t % 32) + 1 and, in each phase, the groups t / 32 + 8 i.  Every global and
+// shared access moves both columns' elements in one 8-byte word, and each twiddle read serves
+// both columns' butterflies (radix_fwd2 / radix_inv2): per butterfly half the memory and twiddle
+// instructions of the one-column form.  GL >= 0: log2 of the row pitch ncols at compile time, so
+// that an element's global address is its group's base plus an immediate.
+constexpr int COL2_TC = 64;
+template <int NB, bool INV, int K, int GL>
+__device__ __forceinline__ void col2_phase(uint32_t* tile, const Tw2* tws, uint32_t* gbase, uint32_t ncols_rt,
+                                           uint32_t p) {
+    using C = LineCfg<NB>;
+    constexpr int b0 = C::b0(K);
+    constexpr int NGRP = (1 << NB) / C::E;  // groups per column
+    constexpr bool FIRST = INV ? K == C::NPH - 1 : K == 0;
+    constexpr bool LAST = INV ? K == 0 : K == C::NPH - 1;
+    const uint32_t ncols = GL >= 0 ? (1u << (GL >= 0 ? GL : 0)) : ncols_rt;
+    const int c2 = 2 * (int)(threadIdx.x & 31);
+    static_assert(NGRP % 8 == 0, "every warp takes whole groups");
+#pragma unroll 1
+    for (int gidx = (int)(threadIdx.x >> 5); gidx < NGRP; gidx += 8) {
+        const int lo = gidx & ((1 << b0) - 1), hip = gidx >> b0;
+        const int xb = (hip << (b0 + C::RB)) | lo;
+        // element e of the group is row xb + (e << b0)
+        uint2* gb = reinterpret_cast<uint2*>(gbase + (size_t)xb * ncols + c2);
+        uint2* sb = reinterpret_cast<uint2*>(tile + xb * COL2_TC + c2);
+        const size_t gstep = ((size_t)ncols << b0) / 2;  // in 8-byte words
+        constexpr int sstep = (COL2_TC << b0) / 2;
+        uint32_t v[C::E], u[C::E];
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) {
+            const uint2 w = FIRST ? gb[e * gstep] : sb[e * sstep];
+            v[e] = w.x;
+            u[e] = w.y;
+        }
+        int tb[C::RB];
+#pragma unroll
+        for (int t = 0; t < C::RB; ++t)
+            tb[t] = INV ? (2 << C::ls(K, t)) - 1 - (hip << t) : (1 << C::ls(K, t)) + (hip << t);
+        if (!INV) {
+            auto stw = [&](int t) { return SmemRun<false>{tws + tb[t], 1 << t}; };
+            radix_fwd2<C::RB, C::t0(K)>(v, u, stw, p);
+        } else {
+            auto stw = [&](int t) { return SmemRun<true>{tws + tb[t] - ((1 << t) - 1), 1 << t}; };
+            radix_inv2<C::RB, C::t0(K)>(v, u, stw, p);
+        }
+#pragma unroll
+        for (int e = 0; e < C::E; ++e) {
+            if (LAST) gb[e * gstep] = make_uint2(v[e], u[e]);
+            else sb[e * sstep] = make_uint2(v[e], u[e]);
+        }
+    }
+}
+
+template <int NB, bool INV, int I, int GL>
+__device__ __forceinline__ void col2_phases(uint32_t* tile, const Tw2* tws, uint32_t* gbase, uint32_t ncols,
+                                            uint32_t p) {
+    using C = LineCfg<NB>;
+    if constexpr (I < C::NPH) {
+        constexpr int K = INV ? C::NPH - 1 - I : I;
+        col2_phase<NB, INV, K, GL>(tile, tws, gbase, ncols, p);
+        if constexpr (I + 1 < C::NPH) {
+            __syncthreads();
+            col2_phases<NB, INV, I + 1, GL>(tile, tws, gbase, ncols, p);
+        }
+    }
+}
+
+template <int NB, bool INV, int GL>
+__global__ void __launch_bounds__(256, 3) k_ntt_cols2(DevPlan P, uint32_t* __restrict__ R, uint32_t col0) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NR = 1 << NB;
+    Tw2* tws = reinterpret_cast<Tw2*>(smem_raw);            // [NR]
+    uint32_t* tile = reinterpret_cast<uint32_t*>(tws + NR);  // [NR][64]
+    const int j = (int)blockIdx.y;
+    const uint32_t p = P.p[j];
+    uint32_t* base = R + ((size_t)blockIdx.z * P.K + j) * P.N + col0 + (blockIdx.x * COL2_TC);
+    const uint2* tw = P.tw + (size_t)j * P.N;
+    pdl_trigger();
+    for (int k = threadIdx.x; k < NR; k += blockDim.x) {
+        const uint2 w = __ldg(tw + k);
+        tws[k] = Tw2{w.x, w.y};
+    }
+    pdl_wait();
+    __syncthreads();
+    col2_phases<NB, INV, 0, GL>(tile, tws, base, P.ncols, p);
+}
+
 template <int NB, bool INV>
 __global__ void __launch_bounds__(256, NB >= 5 ? 4 : 1) k_ntt_cols(DevPlan P, uint32_t* __restrict__ R, uint32_t col0, int ltc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -490,9 +639,35 @@ __global__ void __launch_bounds__(256, NB >= 5 ? 4 : 1) k_ntt_cols(DevPlan P, ui
 
 namespace {
 
+#ifndef POLYMULT_COL2
+#define POLYMULT_COL2 1
+#endif
+// the two-column kernel for a line length 2^NB, row pitch 2^w2 (GL: the pitch at compile time
+// for the splits the tuner tries, w2 in [NB - 1, NB + 1]; else at run time)
+template <int NB, bool INV>
+auto col2_kernel(int w2) {
+    if constexpr (NB >= 7) {
+        if (w2 == NB) return k_ntt_cols2<NB, INV, NB>;
+        if (w2 == NB + 1) return k_ntt_cols2<NB, INV, NB + 1>;
+        if (w2 == NB - 1) return k_ntt_cols2<NB, INV, NB - 1>;
+        return k_ntt_cols2<NB, INV, -1>;
+    } else {
+        return k_ntt_cols2<7, INV, -1>;  // not used (col2_applies)
+    }
+}
+
 template <int NB>
 void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
                     int ltc, bool pdl) {
+    if (POLYMULT_COL2 && NB >= 7 && ltc >= 6) {
+        // 2^ltc columns as 2^(ltc - 6) tiles of 64
+        const dim3 g2(grid.x << (ltc - 6), grid.y, grid.z);
+        const size_t sm2 = ((size_t)8 + 4 * COL2_TC) << NB;
+        const cudaError_t e = launch_kernel(inv ? col2_kernel<NB, true>(P.w2) : col2_kernel<NB, false>(P.w2), g2,
+                                            dim3(256), sm2, s, pdl, P, R, col0);
+        if (e != cudaSuccess) throw_cuda(e, inv ? "launch k_ntt_cols2<inverse>" : "launch k_ntt_cols2<forward>");
+        return;
+    }
     const cudaError_t e = launch_kernel(inv ? k_ntt_cols<NB, true> : k_ntt_cols<NB, false>, grid, dim3(256), smem, s,
                                         pdl, P, R, col0, ltc);
     if (e != cudaSuccess) throw_cuda(e, inv ? "launch k_ntt_cols<inverse>" : "launch k_ntt_cols<forward>");
@@ -542,22 +717,37 @@ struct RowsF {
 };
 template <int NB>
 struct ColAttrF {
-    static void run(int bytes) {
+    static void run(int bytes, int w2) {
         const void* fns[2] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>};
         for (const void* f : fns) {
             const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
             if (e != cudaSuccess) throw_cuda(e, "NTT kernel attribute");
         }
+        if constexpr (NB >= 7) {
+            const void* f2[2] = {(const void*)col2_kernel<NB, false>(w2), (const void*)col2_kernel<NB, true>(w2)};
+            for (const void* f : f2) {
+                const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                if (e != cudaSuccess) throw_cuda(e, "NTT kernel attribute");
+            }
+        }
     }
 };
 template <int NB>
 struct ColProbeF {
-    static void run() {
+    static void run(int w2) {
         const void* fns[2] = {(const void*)k_ntt_cols<NB, false>, (const void*)k_ntt_cols<NB, true>};
         for (const void* f : fns) {
             cudaFuncAttributes fa{};
             const cudaError_t e = cudaFuncGetAttributes(&fa, f);
             if (e != cudaSuccess) throw_cuda(e, "NTT kernel image");
+        }
+        if constexpr (NB >= 7) {
+            const void* f2[2] = {(const void*)col2_kernel<NB, false>(w2), (const void*)col2_kernel<NB, true>(w2)};
+            for (const void* f : f2) {
+                cudaFuncAttributes fa{};
+                const cudaError_t e = cudaFuncGetAttributes(&fa, f);
+                if (e != cudaSuccess) throw_cuda(e, "NTT kernel image");
+            }
         }
     }
 };
@@ -597,16 +787,17 @@ int ntt_rows_per_cta(int w2) {
 }
 
 void ntt_set_smem_limit(int bytes, int w1, int w2) {
-    (void)w2;  // the row kernels use static shared memory only
-    if (w1 > 0) dispatch_nb<ColAttrF>(w1, bytes);
+    // (the row kernels use static shared memory only)
+    if (w1 > 0) dispatch_nb<ColAttrF>(w1, bytes, w2);
 }
 
 void ntt_probe_images(int w1, int w2) {
-    if (w1 > 0) dispatch_nb<ColProbeF>(w1);
+    if (w1 > 0) dispatch_nb<ColProbeF>(w1, w2);
     dispatch_nb<RowProbeF>(w2);
 }
 
 size_t ntt_cols_smem(const DevPlan& P, int ltc) {
+    if (POLYMULT_COL2 && P.w1 >= 7 && ltc >= 6) return ((size_t)8 + 4 * COL2_TC) << P.w1;
     return (size_t)P.nrows * sizeof(Tw2) + ((size_t)P.nrows << ltc) * 4;
 }
 

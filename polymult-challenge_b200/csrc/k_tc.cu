@@ -594,12 +594,20 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 // copies: no register staging, the whole tile in flight at once (register batches
                 // held ~24 KB per SM in flight and left the loads latency-bound); prime slots past
                 // the block's last prime re-read it
+                // The 4 bytes of prime 4g + k land in bank (m & 7) * 4 + k of the row's core matrix
+                // (rows 8 apart are 8 kb bytes apart, a multiple of 128): taken in the order
+                // k = (i + (m >> 3)) & 3, the four rows of a warp that share m & 7 write different
+                // banks at every copy instruction (in the plain order they all hit the same one).
+                // The global side is unchanged: each copy instruction still reads 8-word runs.
+                const int rot = (m >> 3) & 3;
 #pragma unroll 2
                 for (int gg = 0; gg < ng; ++gg) {
                     const int g = g0 + gg;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
+                    for (int i = 0; i < 4; ++i) {
+                        const int k = (i + rot) & 3;
                         cp_async4(arow + (size_t)g * 128 + 4 * k, rp + (size_t)(min(4 * g + k, Kb - 1) - 4 * g0) * N);
+                    }
                 }
                 cp_async_wait_all();
                 // sum y'_j / p_j over this thread's primes, read back from its A row

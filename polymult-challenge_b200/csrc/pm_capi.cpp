@@ -263,11 +263,34 @@ int pm_server_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const 
 }
 
 int pm_server_run(pm_server* server, uint32_t n, const double* t_arrive, const uint32_t* sel,
-                  const uint32_t* const* a, uint32_t* const* c, double* latency, pm_serve_stats* stats) {
+                  const uint32_t* const* a, uint32_t* const* c, double* latency, pm_serve_stats* stats,
+                  uint64_t* digest) {
     if (!server || !server->server) return fail(PM_ERR_INVALID, "null server");
     if (n && (!t_arrive || !sel || !a || !c || !latency)) return fail(PM_ERR_INVALID, "null argument");
-    return guarded([&] { server->server->run(n, t_arrive, sel, a, c, latency, stats); });
+    DeviceScope keep;
+    return guarded([&] { server->server->run(n, t_arrive, sel, a, c, latency, stats, digest); });
 }
+
+int pm_digest(const uint32_t* d_words, uint64_t words, uint32_t count, void* stream, uint64_t* out) {
+    if ((count && !d_words) || (count && !out)) return fail(PM_ERR_INVALID, "null argument");
+    return guarded([&] {
+        if (count == 0) return;
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        uint64_t* d = nullptr;
+        pm::cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&d), (size_t)count * 8, s), "cudaMallocAsync");
+        try {
+            pm::launch_digest(d_words, words, count, d, s);
+            pm::cuda_check(cudaMemcpyAsync(out, d, (size_t)count * 8, cudaMemcpyDeviceToHost, s), "digest D2H");
+            pm::cuda_check(cudaStreamSynchronize(s), "digest");
+        } catch (...) {
+            cudaFreeAsync(d, s);
+            throw;
+        }
+        pm::cuda_check(cudaFreeAsync(d, s), "cudaFreeAsync");
+    });
+}
+
+uint64_t pm_digest_host(const uint32_t* words, uint64_t n) { return words ? pm::digest_host(words, n) : 0; }
 
 int pm_server_host_alloc(pm_server* server, size_t bytes, void** out) {
     if (!server || !server->server || !out) return fail(PM_ERR_INVALID, "null argument");

@@ -303,7 +303,8 @@ uint32_t wait_selftest(int device, long long limit) {
 
 void Engine::setup_launch_shapes() {
     rpb_ = ntt_rows_per_cta(plan_.w2);
-    smem_cols_ = ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(32, plan_.ncols)));
+    smem_cols_ = std::max(ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(32, plan_.ncols))),
+                          ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(64, plan_.ncols))));
     if (smem_cols_ > smem_optin_) throw Unsupported("NTT tile exceeds shared memory");
     // the plain kernels stage their constant tables in shared memory while two blocks still fit
     // an SM (up to W = 1747 or so); beyond that they read them through L1
@@ -770,7 +771,9 @@ void Engine::launch_dec(const uint32_t* src, Chunk ch, uint32_t nb, uint32_t* R,
 
 void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStream_t s, bool pdl) const {
     if (plan_.w1 == 0) return;
-    const int ltc = ilog2(std::min<uint32_t>(32, ch.cw));
+    // tiles of 32 columns (64 for the two-column kernel of lines of >= 128 rows, where the chunk
+    // is at least that wide)
+    const int ltc = ilog2(std::min<uint32_t>(plan_.w1 >= 7 && ch.cw >= 64 ? 64 : 32, ch.cw));
     dim3 grid(ch.cw >> ltc, plan_.K, nb);
     const size_t smem = ntt_cols_smem(dp_, ltc);
     launch_ntt_cols(inv, grid, smem, s, dp_, R, ch.col0, ltc, pdl);

@@ -79,6 +79,11 @@ struct CrtPartial {
 __global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
                          CrtPartial part, CrtPrimeBlocks pbs);
 __global__ void k_crt_finish(DevPlan P, const uint32_t* zp, const float* sp, uint32_t total, uint32_t* out);
+// 64-bit digests of `count` arrays of `words` words (k_digest.cu): out_dev[count] (device) is
+// cleared and filled on stream s; digest_host computes the same value on the host
+void launch_digest(const uint32_t* x, uint64_t words, uint32_t count, uint64_t* out_dev, cudaStream_t s);
+uint64_t digest_host(const uint32_t* x, uint64_t words);
+
 // the bounded waits made to run out (pm_selftest_wait): 64 threads, one block
 __global__ void k_wait_selftest(uint32_t* status, long long limit);
 constexpr long long kWaitClocks = 2000000000ll;  // DevPlan::wait_clocks

@@ -25,6 +25,8 @@
 // loop - arrival time.
 #include "pm_server.h"
 
+#include "pm_kernels.cuh"
+
 #include <algorithm>
 #include <chrono>
 #include <deque>
@@ -67,7 +69,9 @@ Server::Server(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const uint
             s.res = dalloc((size_t)cap_ * rw);
             s.out = dalloc((size_t)cap_ * cw);
             s.sel_d = dalloc(cap_);
+            s.dig_d = reinterpret_cast<uint64_t*>(dalloc(2 * (size_t)cap_));
             cuda_check(cudaHostAlloc(&s.sel_h, cap_ * 4, cudaHostAllocDefault), "cudaHostAlloc");
+            cuda_check(cudaHostAlloc(&s.dig_h, cap_ * 8, cudaHostAllocDefault), "cudaHostAlloc");
         }
         // resident operands -> forward transforms, through slot 0's input buffer
         const Chunk all{0, P.ncols};
@@ -97,6 +101,7 @@ void Server::release() {
         if (s.stream) cudaStreamDestroy(s.stream);
         if (s.done) cudaEventDestroy(s.done);
         if (s.sel_h) cudaFreeHost(s.sel_h);
+        if (s.dig_h) cudaFreeHost(s.dig_h);
     }
     slots_.clear();
     for (void* p : dev_) cudaFree(p);
@@ -121,7 +126,7 @@ void Server::host_free(void* p) {
     host_.erase(it);
 }
 
-void Server::launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint32_t* const* c) {
+void Server::launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint32_t* const* c, bool digest) {
     const Plan& P = eng_->plan();
     const size_t cw = P.coeff_words();
     const uint32_t nb = (uint32_t)s.reqs.size();
@@ -139,6 +144,10 @@ void Server::launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint
     eng_->launch_rows(true, s.res, resident_, nb, s.stream, s.sel_d, true);
     eng_->launch_cols(true, s.res, all, nb, s.stream, true);
     eng_->launch_crt(s.res, all, nb, s.out, s.stream, (size_t)(&s - slots_.data()) * cap_ * P.N, true);
+    if (digest) {
+        launch_digest(s.out, cw, nb, s.dig_d, s.stream);
+        cuda_check(cudaMemcpyAsync(s.dig_h, s.dig_d, nb * 8, cudaMemcpyDeviceToHost, s.stream), "digest D2H");
+    }
     for (uint32_t i = 0; i < nb; ++i)
         cuda_check(cudaMemcpyAsync(c[s.reqs[i]], s.out + i * cw, cw * 4, cudaMemcpyDeviceToHost, s.stream),
                    "result D2H");
@@ -147,7 +156,7 @@ void Server::launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint
 }
 
 void Server::run(uint32_t n, const double* t_arrive, const uint32_t* sel, const uint32_t* const* a,
-                 uint32_t* const* c, double* latency, pm_serve_stats* stats) {
+                 uint32_t* const* c, double* latency, pm_serve_stats* stats, uint64_t* digest) {
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
     for (uint32_t i = 0; i < n; ++i) {
         if (!a[i] || !c[i]) throw InvalidPoint("request " + std::to_string(i) + ": null operand");
@@ -172,6 +181,8 @@ void Server::run(uint32_t n, const double* t_arrive, const uint32_t* sel, const 
                 cuda_check(q, "batch");
                 const double tc = now();
                 for (uint32_t r : s.reqs) latency[r] = tc - t_arrive[r];
+                if (digest)
+                    for (size_t i = 0; i < s.reqs.size(); ++i) digest[s.reqs[i]] = s.dig_h[i];
                 done += (uint32_t)s.reqs.size();
                 inflight -= (uint32_t)s.reqs.size();
                 t_last = tc;
@@ -186,7 +197,7 @@ void Server::run(uint32_t n, const double* t_arrive, const uint32_t* sel, const 
                     s.reqs.push_back(queue.front());
                     queue.pop_front();
                 }
-                launch(s, sel, a, c);
+                launch(s, sel, a, c, digest != nullptr);
                 inflight += nb;
                 peak = std::max(peak, inflight);
                 ++batches;

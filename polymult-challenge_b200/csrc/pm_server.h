@@ -17,8 +17,9 @@ class Server {
     Server(const Server&) = delete;
     Server& operator=(const Server&) = delete;
 
+    // digest: optional; digest[i] receives the device digest (launch_digest) of c[i]
     void run(uint32_t n, const double* t_arrive, const uint32_t* sel, const uint32_t* const* a, uint32_t* const* c,
-             double* latency, pm_serve_stats* stats);
+             double* latency, pm_serve_stats* stats, uint64_t* digest = nullptr);
     void* host_alloc(size_t bytes);
     void host_free(void* p);
 
@@ -36,10 +37,12 @@ class Server {
         uint32_t* out = nullptr;   // [cap][N][L]
         uint32_t* sel_d = nullptr; // [cap] resident index per batch entry
         uint32_t* sel_h = nullptr; // pinned staging of sel_d
+        uint64_t* dig_d = nullptr; // [cap] digests of the batch's results
+        uint64_t* dig_h = nullptr; // pinned copy of dig_d
         std::vector<uint32_t> reqs;
         bool busy = false;
     };
-    void launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint32_t* const* c);
+    void launch(Slot& s, const uint32_t* sel, const uint32_t* const* a, uint32_t* const* c, bool digest);
     void release();
 
     std::unique_ptr<Engine> eng_;

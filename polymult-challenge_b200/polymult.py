@@ -23,7 +23,8 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libpolymult_b200.so")
+# POLYMULT_LIB names another build of the same library (a variant under measurement)
+LIB_PATH = os.environ.get("POLYMULT_LIB") or os.path.join(HERE, "lib", "libpolymult_b200.so")
 HEADER = os.path.join(HERE, "..", "include", "polymult_b200.h")
 
 PM_OK, PM_ERR_INVALID, PM_ERR_CUDA, PM_ERR_DEVICE, PM_ERR_UNSUPPORTED, PM_ERR_INTERNAL = range(6)
@@ -145,7 +146,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                    ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
                                    ctypes.POINTER(vp)]
     lib.pm_server_init.restype = ctypes.c_int
-    lib.pm_server_run.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.POINTER(PmServeStats)]
+    lib.pm_server_run.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.POINTER(PmServeStats), vp]
     lib.pm_server_run.restype = ctypes.c_int
     lib.pm_server_host_alloc.argtypes = [vp, ctypes.c_size_t, ctypes.POINTER(vp)]
     lib.pm_server_host_alloc.restype = ctypes.c_int
@@ -153,6 +154,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_server_host_free.restype = ctypes.c_int
     lib.pm_server_free.argtypes = [vp]
     lib.pm_server_free.restype = None
+    lib.pm_digest.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint32, vp, vp]
+    lib.pm_digest.restype = ctypes.c_int
+    lib.pm_digest_host.argtypes = [vp, ctypes.c_uint64]
+    lib.pm_digest_host.restype = ctypes.c_uint64
     lib.pm_test_fail_scratch_allocs.argtypes = [ctypes.c_int, ctypes.c_int]
     lib.pm_test_fail_scratch_allocs.restype = None
     lib.pm_test_set_status.argtypes = [vp, ctypes.c_uint32]
@@ -182,6 +187,19 @@ def host_pool_selftest(pools: int, runs: int, workers: int = 7, vary: bool = Fal
     flags = (1 if vary else 0) | (2 if park else 0)
     _check(load().pm_selftest_host_pool(pools, runs, workers, flags, ctypes.byref(f)))
     return f.value
+
+
+def digest_device(d_ptr: int, words: int, count: int = 1, stream: int = 0) -> np.ndarray:
+    """pm_digest: 64-bit digests of `count` device arrays of `words` u32 words (contiguous)."""
+    out = np.zeros(count, dtype=np.uint64)
+    _check(load().pm_digest(d_ptr, words, count, stream or None, out.ctypes.data))
+    return out
+
+
+def digest_host(words) -> int:
+    """pm_digest_host: the same digest of a host array."""
+    a = np.ascontiguousarray(words, dtype=np.uint32).reshape(-1)
+    return int(load().pm_digest_host(a.ctypes.data, a.size))
 
 
 def wait_selftest(limit_clocks: int, device: int = 0) -> int:
@@ -370,19 +388,22 @@ class Server:
         buf = (ctypes.c_uint32 * (count * self.N * self.L)).from_address(p.value)
         return np.ctypeslib.as_array(buf).reshape(count, self.N, self.L)
 
-    def run(self, t_arrive, sel, a_bufs, c_bufs):
+    def run(self, t_arrive, sel, a_bufs, c_bufs, digests: bool = False):
         """Plays the request stream; a_bufs[i] / c_bufs[i] are (N, L) u32 host arrays.
-        Returns (latency seconds per request, stats dict)."""
+        Returns (latency seconds per request, stats dict), plus each request's result digest
+        (pm_digest, computed on the device) with digests=True."""
         n = len(t_arrive)
         t = np.ascontiguousarray(t_arrive, dtype=np.float64)
         sv = np.ascontiguousarray(sel, dtype=np.uint32)
         ap = (ctypes.c_void_p * n)(*[x.ctypes.data for x in a_bufs])
         cp = (ctypes.c_void_p * n)(*[x.ctypes.data for x in c_bufs])
         lat = np.zeros(n, dtype=np.float64)
+        dig = np.zeros(n, dtype=np.uint64) if digests else None
         st = PmServeStats()
         _check(load().pm_server_run(self._h, n, t.ctypes.data, sv.ctypes.data, ap, cp, lat.ctypes.data,
-                                    ctypes.byref(st)))
-        return lat, {f: getattr(st, f) for f, _ in PmServeStats._fields_}
+                                    ctypes.byref(st), dig.ctypes.data if digests else None))
+        stats = {f: getattr(st, f) for f, _ in PmServeStats._fields_}
+        return (lat, stats, dig) if digests else (lat, stats)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -84,6 +84,38 @@ def uniform_operands(N: int, W: int, q: int, count: int, seed: int) -> np.ndarra
     return out
 
 
+# the operand distributions of the N=32768, W=868 benchmark configuration
+DISTRIBUTIONS = ("uniform", "all_q_minus_1", "sparse_1pct", "small_16bit")
+
+
+def operands(dist: str, N: int, W: int, q: int, count: int, seed: int) -> np.ndarray:
+    """[count, N, L] u32 limbs drawn from a named distribution (seeded):
+    uniform        coefficients uniform in [0, q);
+    all_q_minus_1  every coefficient q - 1 (the largest input);
+    sparse_1pct    1% of the coefficients (positions drawn without replacement) uniform in
+                   [0, q), the rest 0;
+    small_16bit    coefficients uniform in [0, 2^16)."""
+    L = (W + 31) // 32
+    if dist == "uniform":
+        return uniform_operands(N, W, q, count, seed)
+    if dist == "all_q_minus_1":
+        return np.broadcast_to(limbs(q - 1, L), (count, N, L)).copy()
+    rng = np.random.Generator(np.random.PCG64(seed))
+    if dist == "small_16bit":
+        out = np.zeros((count, N, L), dtype=np.uint32)
+        out[..., 0] = rng.integers(0, 1 << 16, size=(count, N), dtype=np.uint32)
+        return out
+    if dist == "sparse_1pct":
+        out = np.zeros((count, N, L), dtype=np.uint32)
+        nz = max(1, N // 100)
+        vals = uniform_operands(nz, W, q, count, seed + 1)
+        for i in range(count):
+            pos = rng.choice(N, size=nz, replace=False)
+            out[i, pos] = vals[i]
+        return out
+    raise ValueError("unknown distribution %r" % dist)
+
+
 def _load_grid():
     # spec-derived primes of N in {4096..65536} x W in {256, 868, 1747, 3000}, as 2^W - q
     table = {

@@ -112,7 +112,7 @@ def test_batch_server_pipeline_argument_checks():
     assert lib.pm_server_init(64, 256, 8, None, None, 0, 1 << 30, 4, 2, 0, 0, ctypes.byref(out)) == \
         polymult.PM_ERR_INVALID
     assert "resident" in lib.pm_last_error().decode()
-    assert lib.pm_server_run(None, 0, None, None, None, None, None, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_server_run(None, 0, None, None, None, None, None, None, None) == polymult.PM_ERR_INVALID
     lib.pm_server_free(None)
     assert lib.pm_tune_pipeline(None, 3, 0, None) == polymult.PM_ERR_INVALID
     assert lib.pm_tune_pipeline(None, 3, polymult.PIPELINE_PINNED, None) == polymult.PM_ERR_INVALID

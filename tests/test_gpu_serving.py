@@ -103,3 +103,31 @@ def test_hbm_budget_bounds_requests_in_flight():
     with pytest.raises(polymult.PolymultError) as ei:
         polymult.Server(N, W, orc.limbs_of(q, L), res, hbm_budget=fixed + per_req // 2)
     assert ei.value.code == polymult.PM_ERR_INVALID
+
+
+def test_result_digests_match_the_results():
+    """The server's per-request digests (computed on the device before each result's copy)
+    equal the host digest of the result it delivered and of the same product run alone; the
+    standalone device digest (pm_digest) agrees with the host one."""
+    torch = _torch()
+    import polymult
+    ensure_library()
+    N, W = 4096, 868
+    q, L, res, reqs, sel = _setup(N, W, 4, 20, seed=11)
+    want = _alone(torch, N, W, q, L, res, reqs, sel)
+    with polymult.Server(N, W, orc.limbs_of(q, L), res, max_batch=4, streams=3) as srv:
+        a = srv.pinned(len(reqs))
+        c = srv.pinned(len(reqs))
+        a[:] = reqs
+        lat, st, dig = srv.run(np.zeros(len(reqs)), sel, list(a), list(c), digests=True)
+        got = np.array(c)
+    assert np.array_equal(got, want)
+    for i in range(len(reqs)):
+        assert int(dig[i]) == polymult.digest_host(got[i]) == polymult.digest_host(want[i]), i
+    d = torch.from_numpy(np.ascontiguousarray(want).view(np.int32)).cuda()
+    dd = polymult.digest_device(d.data_ptr(), N * L, len(reqs))
+    assert [int(x) for x in dd] == [polymult.digest_host(w) for w in want]
+    # a one-word change moves the digest
+    w2 = want[0].copy()
+    w2[N // 2, 3] ^= 1
+    assert polymult.digest_host(w2) != polymult.digest_host(want[0])
