@@ -352,6 +352,29 @@ def pcie_bandwidth(torch, nbytes_h2d, nbytes_d2h, reps=5):
     return out
 
 
+def host_copy_gbs(torch, nbytes, threads=8, reps=5):
+    """Host memory copy rate pageable -> page-locked (the pageable call's staging copy) with
+    `threads` threads, best of `reps`, in GB/s."""
+    import numpy as np
+    words = nbytes // 4
+    src = np.random.default_rng(3).integers(0, 2**32, size=words, dtype=np.uint32)
+    dst = torch.empty(words, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    parts = np.array_split(np.arange(words), threads)
+
+    def work(p):
+        np.copyto(dst[p[0]:p[-1] + 1], src[p[0]:p[-1] + 1])
+    best = float("inf")
+    for _ in range(reps):
+        ts = [threading.Thread(target=work, args=(p,)) for p in parts]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        best = min(best, time.perf_counter() - t0)
+    return nbytes / best / 1e9
+
+
 def pcie_floor_ms(bw, N, L):
     return (2 * N * L * 4 / (bw["h2d"] * 1e9) + N * L * 4 / (bw["d2h"] * 1e9)) * 1000
 
@@ -424,9 +447,12 @@ def run_configs(torch, args, local, pending):
                 mt = polymult.Multiplier(N, W, qv, gemm="tensor", device=local)
                 mp = polymult.Multiplier(N, W, qv, gemm="plain", device=local)
                 bw = pcie_bandwidth(torch, 2 * N * L * 4, N * L * 4)
-                pipe = mt.tune_pipeline(3, pinned=True) if not args.no_tune_pipeline else mt.pipeline(pinned=True)
-                engines[(N, W)] = (mt, mp, bw, pipe)
-            mt, mp, bw, pipe = engines[(N, W)]
+                if args.no_tune_pipeline:
+                    pipe, pipe_pg = mt.pipeline(pinned=True), mt.pipeline()
+                else:
+                    pipe, pipe_pg = mt.tune_pipeline(3, pinned=True), mt.tune_pipeline(3)
+                engines[(N, W)] = (mt, mp, bw, pipe, pipe_pg)
+            mt, mp, bw, pipe, pipe_pg = engines[(N, W)]
             B = min(int(mt.info()["group"]), 32)
             ops = workload.operands(dist, N, W, q, 2 * B, seed=500 + ci)
             a_h, b_h = np.ascontiguousarray(ops[:B]), np.ascontiguousarray(ops[B:])
@@ -461,12 +487,12 @@ def run_configs(torch, args, local, pending):
                 "tensor_over_plain": round((steps * B / ms_t) / (max(3, nsets) * B / ms_p), 3),
                 "e2e_pinned": e2e_pinned, "e2e_pageable": e2e_pageable,
                 "pcie_floor_ms": round(floor_ms, 4), "pcie_gbs": {k: round(v, 2) for k, v in bw.items()},
-                "chunk_schedule_pinned": pipe,
+                "chunk_schedule_pinned": pipe, "chunk_schedule_pageable": pipe_pg,
                 "forms_agree": bool(np.array_equal(res_t, res_p)),
                 "matches_reference": None}  # filled in by the cpu_baseline leg
             del sets, da0, db0, ct
     finally:
-        for mt, mp, _, _ in engines.values():
+        for mt, mp, _, _, _ in engines.values():
             mt.close()
             mp.close()
     torch.cuda.empty_cache()
@@ -807,6 +833,12 @@ def run_ours(args):
     e2e["pageable"] = e2e_leg(m, np.ascontiguousarray(host_a[0]), np.ascontiguousarray(host_b[0]),
                               np.empty((N, L), dtype=np.uint32), args.e2e_steps, world, floor_ms, want)
     e2e["pageable"]["chunk_schedule"] = pipe_pageable
+    # the pageable call's second floor: its host copies (a and b gathered into page-locked
+    # staging, c scattered out of it) at the host's measured copy rate with the pool's 8 threads
+    hbw = host_copy_gbs(torch, 2 * N * L * 4)
+    host_floor = 3 * N * L * 4 / (hbw * 1e9) * 1000
+    e2e["pageable"].update({"host_copy_gbs": round(hbw, 1), "host_staging_floor_ms": round(host_floor, 4),
+                            "p50_over_host_floor": round(e2e["pageable"]["p50_ms"] / host_floor, 3)})
     m.close()
     mp.close()
     del sets, da, db, dc, dc2

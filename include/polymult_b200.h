@@ -217,11 +217,13 @@ typedef struct pm_pipeline_info {
 #define PM_PIPELINE_PINNED 1
 
 /* No reference counterpart: the autotuner of the host pipeline.  Runs `reps` pm_run calls (plus
- * a warm-up) for every schedule with body divisors in {4, 8, 16} x {4, 8, 16} on pageable
- * timing buffers (with PM_PIPELINE_PINNED: {2, 3, 4, 8, 16} x {2, 3, 4, 8, 16} on page-locked
- * ones; 3 stands for the chunks 1/2, 1/4, 1/4 of b and 1/4, 1/4, 1/2 of c), keeps the one with the
- * lowest median wall time for that kind of call, and describes it in *out.  Synchronous; about
- * 10 (PM_PIPELINE_PINNED: 26) x (reps + 1) calls. */
+ * a warm-up) for every schedule with body divisors in {1, 2, 4, 8, 16} x {1, 2, 4, 8, 16} on
+ * pageable timing buffers (narrow head chunks only with a body of 8 or more; with
+ * PM_PIPELINE_PINNED: {1, 2, 3, 4, 8, 16} squared on page-locked ones, 3 standing for the chunks
+ * 1/2, 1/4, 1/4 of b and 1/4, 1/4, 1/2 of c), keeps the one with the lowest median wall time for
+ * that kind of call, and describes it in *out.  Before any tuning the schedules follow the
+ * operand size (one chunk below 1 MB, quarters below 8 MB, eighths above).  Synchronous; up to
+ * 25 (PM_PIPELINE_PINNED: 36) x (reps + 1) calls. */
 int pm_tune_pipeline(pm_context* ctx, int reps, int flags, pm_pipeline_info* out);
 int pm_get_pipeline(const pm_context* ctx, int flags, pm_pipeline_info* out);
 

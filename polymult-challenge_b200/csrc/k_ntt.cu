@@ -54,7 +54,7 @@ __device__ __forceinline__ void radix_fwd(uint32_t (&v)[1 << RB], const StwF& st
             const Tw2 wm = w[m];
 #pragma unroll
             for (int i = 0; i < h; ++i) {
-                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p, m * h + i);
+                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
             }
         }
     }
@@ -74,8 +74,8 @@ __device__ __forceinline__ void radix_fwd2(uint32_t (&v)[1 << RB], uint32_t (&u)
             const Tw2 wm = w[m];
 #pragma unroll
             for (int i = 0; i < h; ++i) {
-                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p, 0);
-                bfly_ct_sh(u[m * 2 * h + i], u[m * 2 * h + i + h], wm, p, 1);
+                bfly_ct_sh(v[m * 2 * h + i], v[m * 2 * h + i + h], wm, p);
+                bfly_ct_sh(u[m * 2 * h + i], u[m * 2 * h + i + h], wm, p);
             }
         }
     }
@@ -160,9 +160,6 @@ struct SmemRun {
 // so that every exchange of the phase layouts below is free of bank conflicts -- with
 // 16-byte vector access in the last phase for NB = 6, 7, 8.
 // ---------------------------------------------------------------------------------------
-#ifndef POLYMULT_ROW_LAYOUT
-#define POLYMULT_ROW_LAYOUT 0
-#endif
 template <int NB>
 struct RowCfg : LineCfg<NB> {
     using B = LineCfg<NB>;
@@ -171,17 +168,7 @@ struct RowCfg : LineCfg<NB> {
     static constexpr int RPG = GRP / LPR;             // rows per shared-memory region
     static constexpr int ROWS_PER_CTA = 128 / LPR;   // 128 threads per CTA
     static constexpr bool VEC = NB >= 6 && NB <= 8;   // swizzle keeps runs of 4 contiguous
-    // Additive layout (NB = 7, 8): element x of region row rho at rho * RS + x + 4 (x >> 4) -- each
-    // 16-element segment padded to 20 words, the row stride RS chosen so that the rows of a warp
-    // start 32 / RPG banks apart.  Every access of a phase is then the thread's base plus a
-    // compile-time offset (an immediate in the instruction, no address arithmetic), and both
-    // exchanges are conflict-free: a scalar phase's 32 lanes cover 32 consecutive banks (row
-    // offsets 16 (NB = 8) or 8 (NB = 7) apart, lanes of a row consecutive), and a vector phase's
-    // quarter-warps (one row's 8 segments) start at 20 r mod 32 = {0, 20, 8, 28, 16, 4, 24, 12}.
-    static constexpr bool ADD = POLYMULT_ROW_LAYOUT && (NB == 7 || NB == 8);
-    static constexpr int RS = NB == 8 ? 336 : 168;
-    static constexpr int REGION = ADD ? RPG * RS : GRP * B::E;  // words per region
-    __host__ __device__ static constexpr int pos(int rho, int x) { return rho * RS + x + 4 * (x >> 4); }
+    static constexpr int REGION = GRP * B::E;         // words per region
     __host__ __device__ static constexpr uint32_t g(int i) {
         // G(input bit i of X >> 5) for each NB; NB <= 4 has a single phase and no exchange
         return NB == 5 || NB == 9 ? (i == 0 ? 2u : i == 1 ? 4u : i == 2 ? 8u : i == 3 ? 17u : 0u)
@@ -218,33 +205,6 @@ template <int NB, int K, bool TO_SMEM>
 __device__ __forceinline__ void row_xchg(uint32_t (&v)[RowCfg<NB>::E], uint32_t* region, int rho, int r) {
     using C = RowCfg<NB>;
     constexpr int b0 = C::b0(K);
-    if constexpr (C::ADD) {
-        // x(e) = x(0) + (e << b0) with disjoint bits, and x >> 4 splits the same way, so
-        // pos(rho, x(e)) = pos(rho, x(0)) + pos(0, e << b0) (for b0 = 0, e stays inside x(0)'s segment)
-        uint32_t* base = region + C::pos(rho, row_x<NB, K>(r, 0));
-        if constexpr (b0 == 0) {
-#pragma unroll
-            for (int q = 0; q < C::E / 4; ++q) {
-                uint4* a = reinterpret_cast<uint4*>(base + 4 * q);
-                if (TO_SMEM) *a = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-                else {
-                    const uint4 u = *a;
-                    v[4 * q] = u.x;
-                    v[4 * q + 1] = u.y;
-                    v[4 * q + 2] = u.z;
-                    v[4 * q + 3] = u.w;
-                }
-            }
-        } else {
-#pragma unroll
-            for (int e = 0; e < C::E; ++e) {
-                uint32_t* a = base + C::pos(0, e << b0);
-                if (TO_SMEM) *a = v[e];
-                else v[e] = *a;
-            }
-        }
-        return;
-    }
     // the register bits of X are zero in the base: X(e) = base ^ (e << b0)
     const int sbase = C::swz((rho << NB) | row_x<NB, K>(r, 0));
     if constexpr (C::VEC && b0 == 0) {
@@ -529,7 +489,8 @@ __device__ __forceinline__ void col_phases(uint32_t* tile, const Tw2* tws, uint3
 
 }  // namespace
 
-// Two-column form (lines of 2^NB >= 128 rows, tiles of 64 columns): thread t owns columns
+// Two-column form (lines of 128 or 256 rows, tiles of 64 columns: 33 / 66 KB of shared memory,
+// three CTAs per SM at 256 rows; longer lines keep the one-column form): thread t owns columns
 // 2 (t % 32) and 2 (t % 32) + 1 and, in each phase, the groups t / 32 + 8 i.  Every global and
 // shared access moves both columns' elements in one 8-byte word, and each twiddle read serves
 // both columns' butterflies (radix_fwd2 / radix_inv2): per butterfly half the memory and twiddle
@@ -646,7 +607,7 @@ namespace {
 // for the splits the tuner tries, w2 in [NB - 1, NB + 1]; else at run time)
 template <int NB, bool INV>
 auto col2_kernel(int w2) {
-    if constexpr (NB >= 7) {
+    if constexpr (NB >= 7 && NB <= 8) {
         if (w2 == NB) return k_ntt_cols2<NB, INV, NB>;
         if (w2 == NB + 1) return k_ntt_cols2<NB, INV, NB + 1>;
         if (w2 == NB - 1) return k_ntt_cols2<NB, INV, NB - 1>;
@@ -659,7 +620,7 @@ auto col2_kernel(int w2) {
 template <int NB>
 void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevPlan& P, uint32_t* R, uint32_t col0,
                     int ltc, bool pdl) {
-    if (POLYMULT_COL2 && NB >= 7 && ltc >= 6) {
+    if (POLYMULT_COL2 && NB >= 7 && NB <= 8 && ltc >= 6) {
         // 2^ltc columns as 2^(ltc - 6) tiles of 64
         const dim3 g2(grid.x << (ltc - 6), grid.y, grid.z);
         const size_t sm2 = ((size_t)8 + 4 * COL2_TC) << NB;
@@ -723,7 +684,7 @@ struct ColAttrF {
             const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
             if (e != cudaSuccess) throw_cuda(e, "NTT kernel attribute");
         }
-        if constexpr (NB >= 7) {
+        if constexpr (NB >= 7 && NB <= 8) {
             const void* f2[2] = {(const void*)col2_kernel<NB, false>(w2), (const void*)col2_kernel<NB, true>(w2)};
             for (const void* f : f2) {
                 const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -741,7 +702,7 @@ struct ColProbeF {
             const cudaError_t e = cudaFuncGetAttributes(&fa, f);
             if (e != cudaSuccess) throw_cuda(e, "NTT kernel image");
         }
-        if constexpr (NB >= 7) {
+        if constexpr (NB >= 7 && NB <= 8) {
             const void* f2[2] = {(const void*)col2_kernel<NB, false>(w2), (const void*)col2_kernel<NB, true>(w2)};
             for (const void* f : f2) {
                 cudaFuncAttributes fa{};
@@ -797,7 +758,7 @@ void ntt_probe_images(int w1, int w2) {
 }
 
 size_t ntt_cols_smem(const DevPlan& P, int ltc) {
-    if (POLYMULT_COL2 && P.w1 >= 7 && ltc >= 6) return ((size_t)8 + 4 * COL2_TC) << P.w1;
+    if (POLYMULT_COL2 && P.w1 >= 7 && P.w1 <= 8 && ltc >= 6) return ((size_t)8 + 4 * COL2_TC) << P.w1;
     return (size_t)P.nrows * sizeof(Tw2) + ((size_t)P.nrows << ltc) * 4;
 }
 

@@ -789,45 +789,22 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
                 }
                 continue;
             }
-            // coalesced store of the tile's cnt x L limbs (contiguous in the output); element w =
-            // row mm, limb col, tracked incrementally (each sweep advances w by qL rows + rL
-            // limbs).  With a 16-byte aligned run, 4 consecutive words per thread and sweep.
+            // coalesced store of the tile's cnt x L limbs (contiguous in the output): thread et takes
+            // words et, et + 256, ...; word w is limb col of row mm, tracked incrementally (each sweep
+            // advances w by qL rows + rL limbs).  Consecutive threads read consecutive limbs of the
+            // odd-stride rows of S.z, so the loads spread over all banks (four consecutive words per
+            // thread, for 16-byte stores, put the threads 8 apart on one bank).
             uint32_t* o = out + ((size_t)bt * npos + pos0) * L;
             const int tot = cnt * L;
-            if (((uintptr_t)o & 15) == 0 && (tot & 3) == 0) {
-                constexpr int step = 4 * CRT_EPI_THREADS;
-                const int qL = step / L, rL = step - qL * L;
-                int mm = (4 * et) / L, col = 4 * et - mm * L;
-                for (int w = 4 * et; w < tot; w += step) {
-                    uint32_t v4[4];
-                    int m2 = mm, c2 = col;
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        v4[k] = S.z[(size_t)m2 * zs + c2];
-                        if (++c2 == L) {
-                            c2 = 0;
-                            ++m2;
-                        }
-                    }
-                    *reinterpret_cast<uint4*>(o + w) = make_uint4(v4[0], v4[1], v4[2], v4[3]);
-                    mm += qL;
-                    col += rL;
-                    if (col >= L) {
-                        col -= L;
-                        ++mm;
-                    }
-                }
-            } else {
-                const int qL = CRT_EPI_THREADS / L, rL = CRT_EPI_THREADS - qL * L;
-                int mm = et / L, col = et - mm * L;
-                for (int w = et; w < tot; w += CRT_EPI_THREADS) {
-                    o[w] = S.z[(size_t)mm * zs + col];
-                    mm += qL;
-                    col += rL;
-                    if (col >= L) {
-                        col -= L;
-                        ++mm;
-                    }
+            const int qL = CRT_EPI_THREADS / L, rL = CRT_EPI_THREADS - qL * L;
+            int mm = et / L, col = et - mm * L;
+            for (int w = et; w < tot; w += CRT_EPI_THREADS) {
+                o[w] = S.z[(size_t)mm * zs + col];
+                mm += qL;
+                col += rL;
+                if (col >= L) {
+                    col -= L;
+                    ++mm;
                 }
             }
         }

@@ -91,7 +91,8 @@ __device__ __forceinline__ uint32_t redc64(uint64_t t, uint32_t p, uint32_t pinv
     return (uint32_t)(t >> 32) - __umulhi(m, p) + p;
 }
 
-// [0, 2m) -> [0, m) (also [0, 4p) -> [0, 2p) with m = 2p): unsigned min of x and x - m.
+// [0, 2m) -> [0, m) (also [0, 4p) -> [0, 2p) with m = 2p): unsigned min of x and x - m (one
+// fused add-and-min instruction on this architecture).
 __device__ __forceinline__ uint32_t red_once(uint32_t x, uint32_t m) { return min(x, x - m); }
 
 // A twiddle in Shoup form: w < p and wc = floor(w 2^32 / p).
@@ -106,35 +107,13 @@ __device__ __forceinline__ uint32_t mul_sh(uint32_t x, uint32_t w, uint32_t wsh,
 }
 
 // Cooley-Tukey butterfly with a Shoup twiddle {w, wsh}: x, y in [0, 4p) -> [0, 4p).
-// Two forms of the same arithmetic (mod 2^32 throughout, every true value in range):
-//   A: t = y w - q p, x' = xr + t, y' = xr - t + 2p         (3 multiplies, 4 adds / min)
-//   B: x' = xr + y w - q p (two multiply-adds), y' = 2 xr + 2p - x'
-// The integer ALU pipe and the multiply-add pipe each take half a warp instruction per cycle
-// per scheduler; A puts 4 of 7 instructions on the ALU pipe, B moves an add onto the
-// multiply-add pipe.  POLYMULT_BFLY: 0 = A everywhere, 1 = B everywhere, 2 = alternating
-// (the ALU and multiply-add pipes equally loaded on average).
-#ifndef POLYMULT_BFLY
-#define POLYMULT_BFLY 0
-#endif
-__device__ __forceinline__ void bfly_ct_form_a(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
+// Three multiplies (one high) and three adds / one fused add-and-min.
+__device__ __forceinline__ void bfly_ct_sh(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
     const uint32_t p2 = 2 * p;
     const uint32_t xr = red_once(x, p2);
     const uint32_t t = mul_sh(y, w.w, w.wc, p);
     x = xr + t;
     y = xr - t + p2;
-}
-__device__ __forceinline__ void bfly_ct_form_b(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p) {
-    const uint32_t p2 = 2 * p;
-    const uint32_t xr = red_once(x, p2);
-    const uint32_t q = __umulhi(y, w.wc);
-    const uint32_t xn = xr + y * w.w - q * p;
-    y = 2 * xr + p2 - xn;
-    x = xn;
-}
-// `slot`: the butterfly's position in its (fully unrolled) network, a compile-time constant there
-__device__ __forceinline__ void bfly_ct_sh(uint32_t& x, uint32_t& y, Tw2 w, uint32_t p, int slot = 0) {
-    if (POLYMULT_BFLY == 1 || (POLYMULT_BFLY == 2 && (slot & 1))) bfly_ct_form_b(x, y, w, p);
-    else bfly_ct_form_a(x, y, w, p);
 }
 
 // Gentleman-Sande (inverse) butterfly with the mirrored Shoup twiddle: x, y in [0, 2p) ->

@@ -303,8 +303,10 @@ uint32_t wait_selftest(int device, long long limit) {
 
 void Engine::setup_launch_shapes() {
     rpb_ = ntt_rows_per_cta(plan_.w2);
+    // the widest tile launch_cols uses: 64 columns for lines of 128 or 256 rows, else 32
+    const uint32_t widest = plan_.w1 >= 7 && plan_.w1 <= 8 ? 64 : 32;
     smem_cols_ = std::max(ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(32, plan_.ncols))),
-                          ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(64, plan_.ncols))));
+                          ntt_cols_smem(dp_, ilog2(std::min<uint32_t>(widest, plan_.ncols))));
     if (smem_cols_ > smem_optin_) throw Unsupported("NTT tile exceeds shared memory");
     // the plain kernels stage their constant tables in shared memory while two blocks still fit
     // an SM (up to W = 1747 or so); beyond that they read them through L1
@@ -400,8 +402,10 @@ void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind) {
         throw InvalidPoint("chunk divisors must be powers of two (or 3 for direct-copy calls)");
     const uint32_t nc = plan_.ncols;
     if (kind == 0) {
-        cin_[kind] = make_chunks(nc, {32, 32, 16}, in_body, {});
-        cout_[kind] = make_chunks(nc, {64, 32}, out_body, {32, 64});
+        // narrow head (and output tail) chunks only under a fine body: they start the staging
+        // sooner, but each chunk costs its own copy set-up and launches
+        cin_[kind] = in_body >= 8 ? make_chunks(nc, {32, 32, 16}, in_body, {}) : make_chunks(nc, {}, in_body, {});
+        cout_[kind] = out_body >= 8 ? make_chunks(nc, {64, 32}, out_body, {32, 64}) : make_chunks(nc, {}, out_body, {});
     } else {
         cin_[kind] = in_body == 3 ? make_chunks(nc, {2}, 4, {}) : make_chunks(nc, {}, in_body, {});
         cout_[kind] = out_body == 3 ? make_chunks(nc, {}, 4, {2}) : make_chunks(nc, {}, out_body, {});
@@ -452,12 +456,12 @@ double Engine::tune_host_pipeline(int reps, int kind) {
     // body divisors: 4, 8, 16; direct-copy calls also 2 and 3 (fewer copies, each ~4 us of DMA
     // set-up, against more compute exposed after the last input chunk and before the first output
     // one; 3: the uneven three-chunk shapes of set_chunk_schedule)
-    const uint32_t cand[5] = {2, 3, 4, 8, 16};
+    const uint32_t cand[6] = {1, 2, 3, 4, 8, 16};
     try {
         for (uint32_t ib : cand)
             for (uint32_t ob : cand) {
                 if (ib > plan_.ncols || ob > plan_.ncols) continue;
-                if (kind == 0 && (ib < 4 || ob < 4)) continue;
+                if (kind == 0 && (ib == 3 || ob == 3)) continue;
                 set_chunk_schedule(ib, ob, kind);
                 run_host(a, a, c);
                 std::vector<double> t;
@@ -505,8 +509,13 @@ void Engine::setup_host_pipeline() {
     for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
-    set_chunk_schedule(8, 8, 0);
-    set_chunk_schedule(8, 8, 1);
+    // default schedules by operand size (the tuner refines them): a point of a few hundred KB
+    // moves in one chunk each way (its copies take microseconds, each chunk costs a few of set-up
+    // and four launches), a few MB in quarters, larger points in eighths with narrow heads
+    const size_t opb = plan_.coeff_words() * 4;
+    const uint32_t body = opb < (1u << 20) ? 1 : opb < (8u << 20) ? 4 : 8;
+    set_chunk_schedule(std::min<uint32_t>(body, plan_.ncols), std::min<uint32_t>(body, plan_.ncols), 0);
+    set_chunk_schedule(std::min<uint32_t>(body, plan_.ncols), std::min<uint32_t>(body, plan_.ncols), 1);
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
     // 8 copying threads (7 workers + the caller) by default.  On the 16-CPU B200 hosts measured,
     // 12 threads stage an operand pair faster in isolation (0.63 ms against 1.0 ms) but made the
@@ -773,7 +782,7 @@ void Engine::launch_cols(bool inv, uint32_t* R, Chunk ch, uint32_t nb, cudaStrea
     if (plan_.w1 == 0) return;
     // tiles of 32 columns (64 for the two-column kernel of lines of >= 128 rows, where the chunk
     // is at least that wide)
-    const int ltc = ilog2(std::min<uint32_t>(plan_.w1 >= 7 && ch.cw >= 64 ? 64 : 32, ch.cw));
+    const int ltc = ilog2(std::min<uint32_t>(plan_.w1 >= 7 && plan_.w1 <= 8 && ch.cw >= 64 ? 64 : 32, ch.cw));
     dim3 grid(ch.cw >> ltc, plan_.K, nb);
     const size_t smem = ntt_cols_smem(dp_, ltc);
     launch_ntt_cols(inv, grid, smem, s, dp_, R, ch.col0, ltc, pdl);
@@ -980,8 +989,21 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     ensure_scratch(1);
     const uint32_t nrows = plan_.nrows, ncols = plan_.ncols, L = plan_.L;
     const uint32_t* src[2] = {a, b};
-    const uint32_t ntasks = std::min<uint32_t>(nrows, 64);
-    const uint32_t rpt = (nrows + ntasks - 1) / ntasks;
+    // staging tasks of at least 128 KB of the chunk each (up to 64, one per row at most): a small
+    // chunk is copied by the calling thread alone rather than handed to the pool
+    auto tasks_for = [&](uint32_t cw) {
+        const size_t bytes = (size_t)nrows * cw * L * 4;
+        return (uint32_t)std::max<size_t>(1, std::min<size_t>({(size_t)nrows, 64, bytes >> 17}));
+    };
+    auto staged_copy = [&](uint32_t cw, const std::function<void(uint32_t)>& row_copy) {
+        const uint32_t nt = tasks_for(cw), rpt = (nrows + nt - 1) / nt;
+        auto task = [&](int t) {
+            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
+            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r) row_copy(r);
+        };
+        if (nt == 1) task(0);
+        else pool_->run((int)nt, task);
+    };
     // operands already in page-locked memory skip the host staging: each column chunk moves
     // with one strided DMA copy (rows of cw * L words at a pitch of ncols * L words); with all
     // three page-locked the call runs the direct-copy schedule
@@ -1008,10 +1030,8 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         const Chunk ch = items[i].second;
         uint32_t* dst = h_in_[P] + (size_t)ch.col0 * nrows * L;
         const size_t seg = (size_t)ch.cw * L;
-        pool_->run((int)ntasks, [&](int t) {
-            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
-            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r)
-                stream_copy(dst + r * seg, src[P] + ((size_t)r * ncols + ch.col0) * L, seg * 4, nt_gather_);
+        staged_copy(ch.cw, [&](uint32_t r) {
+            stream_copy(dst + r * seg, src[P] + ((size_t)r * ncols + ch.col0) * L, seg * 4, nt_gather_);
         });
     };
     uint32_t* dR[2] = {d_ra_, d_rb_};
@@ -1111,10 +1131,8 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
         const Chunk ch = cout[oc];
         const uint32_t* srcc = h_out_ + (size_t)ch.col0 * nrows * L;
         const size_t seg = (size_t)ch.cw * L;
-        pool_->run((int)ntasks, [&](int t) {
-            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
-            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r)
-                stream_copy(c + ((size_t)r * ncols + ch.col0) * L, srcc + r * seg, seg * 4);
+        staged_copy(ch.cw, [&](uint32_t r) {
+            stream_copy(c + ((size_t)r * ncols + ch.col0) * L, srcc + r * seg, seg * 4);
         });
     }
     if (profile_) {

@@ -6,7 +6,8 @@ N=65536/W=1747) is run through both entry points (host operands: pm_run, the ref
 fherma_run; device operands: pm_run_device) in both GEMM forms (CUDA-core plain, tcgen05
 tensor-core) and compared byte-for-byte with c.bin as the reference's tests/oracle.py wrote
 it.  Beyond the golden set: batched device calls, random operands at the ranked point
-against the C oracle, repeatability, and the device status word."""
+against the C oracle, repeatability, and a clean device status word after every run (pm_sync);
+the status word's failure reports themselves are driven in test_gpu_failures.py."""
 import numpy as np
 import pytest
 
@@ -171,15 +172,17 @@ def test_tuned_pipeline_still_bit_exact():
     results stay byte-identical to the reference's and the schedule is one of the candidates."""
     pt = next(p for p in POINTS if (p["N"], p["W"]) == (32768, 868))
     with _multiplier(pt, "tensor") as m:
+        # before tuning the schedule follows the operand size: 3.7 MB per operand -> quarters
         before = m.pipeline()
-        assert before["in_body"] == 8 and before["out_body"] == 8 and before["tuned_ms"] == 0
+        assert before["in_body"] == 4 and before["out_body"] == 4 and before["tuned_ms"] == 0
         info = m.tune_pipeline(2)
-        assert info["in_body"] in (4, 8, 16) and info["out_body"] in (4, 8, 16) and info["tuned_ms"] > 0
+        assert info["in_body"] in (1, 2, 4, 8, 16) and info["out_body"] in (1, 2, 4, 8, 16) and info["tuned_ms"] > 0
         assert m.pipeline() == info
         # the page-locked schedule is tuned on its own and leaves the staged one alone
         assert m.pipeline(pinned=True)["tuned_ms"] == 0
         pinfo = m.tune_pipeline(2, pinned=True)
-        assert pinfo["in_body"] in (2, 3, 4, 8, 16) and pinfo["out_body"] in (2, 3, 4, 8, 16) and pinfo["tuned_ms"] > 0
+        assert pinfo["in_body"] in (1, 2, 3, 4, 8, 16) and pinfo["out_body"] in (1, 2, 3, 4, 8, 16)
+        assert pinfo["tuned_ms"] > 0
         assert m.pipeline(pinned=True) == pinfo and m.pipeline() == info
         for case in pt["cases"]:
             a, b, _ = regen_case(pt, case)
