@@ -362,31 +362,50 @@ enum : int { ROWS_FWD = 0, ROWS_FUSED = 1, ROWS_BOTH = 2 };
 __host__ __device__ constexpr int rows_min_blocks(int nb, int mode) {
     return nb >= 9 ? (mode == ROWS_FWD ? 5 : 4) : (mode == ROWS_FWD ? 8 : 6);
 }
-template <int NB, int MODE>
+// POLYMULT_ROW_STATIC: the row kernels take the column-stage count w1 (and with it nrows and N)
+// as a template constant for the common splits, and a grid ordered (batch, row block, prime) so
+// that the block's indices need no division (row pass of both operands at N=65536, W=1747:
+// 34.2 -> 32.8 us per multiply, N=32768, W=868: 9.47 -> 9.03); otherwise w1 from the plan and a
+// (row block, prime, batch) grid linearised batch entry fastest.
+#ifndef POLYMULT_ROW_STATIC
+#define POLYMULT_ROW_STATIC 1
+#endif
+template <int NB, int MODE, int W1>
 __global__ void __launch_bounds__(128, rows_min_blocks(NB, MODE)) k_ntt_rows(DevPlan P, uint32_t* __restrict__ R,
                                                                            const uint32_t* __restrict__ RA,
                                                                            const uint32_t* __restrict__ ra_sel) {
     using C = RowCfg<NB>;
+    const int w1 = W1 >= 0 ? W1 : P.w1;
+    const uint32_t nrows = W1 >= 0 ? (1u << (W1 >= 0 ? W1 : 0)) : P.nrows;
+    const uint32_t Nn = W1 >= 0 ? (1u << ((W1 >= 0 ? W1 : 0) + NB)) : P.N;  // N <= 2^20
     constexpr int REGION_WORDS = C::NPH > 1 ? (128 / C::GRP) * C::REGION : 4;  // one operand's regions
     __shared__ __align__(16) uint32_t sh[MODE == ROWS_BOTH ? 2 * REGION_WORDS : REGION_WORDS];
     const int tid = threadIdx.x;
     const int li = tid % C::GRP;                 // thread within the shared-memory region
     const int rho = li / C::LPR, r = li % C::LPR;
     uint32_t* region = sh + (tid / C::GRP) * C::REGION;
-    // the grid is (row blocks, primes, batch); blocks take them batch entry fastest in launch
-    // order, so the nb blocks of one (row block, prime), which read the same twiddles, run
-    // side by side and share them in L2
-    const uint32_t lin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    const uint32_t zb = lin % gridDim.z, rest = lin / gridDim.z;
-    const uint32_t xb = rest % gridDim.x;
-    const int j = (int)(rest / gridDim.x);
+    // blocks run batch entry fastest in launch order, so the nb blocks of one (row block, prime),
+    // which read the same twiddles, run side by side and share them in L2
+    uint32_t zb, xb;
+    int j;
+    if (POLYMULT_ROW_STATIC) {  // grid (batch, row blocks, primes)
+        zb = blockIdx.x;
+        xb = blockIdx.y;
+        j = (int)blockIdx.z;
+    } else {  // grid (row blocks, primes, batch), linearised
+        const uint32_t lin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        zb = lin % gridDim.z;
+        const uint32_t rest = lin / gridDim.z;
+        xb = rest % gridDim.x;
+        j = (int)(rest / gridDim.x);
+    }
     const uint32_t hi = xb * C::ROWS_PER_CTA + (uint32_t)(tid / C::LPR);
-    const bool active = hi < P.nrows;
-    const uint32_t hic = active ? hi : P.nrows - 1;  // keeps twiddle reads in range
+    const bool active = hi < nrows;
+    const uint32_t hic = active ? hi : nrows - 1;  // keeps twiddle reads in range
     const uint32_t p = P.p[j], pinv = P.pinv[j];
-    const size_t off = ((size_t)zb * P.K + j) * P.N + (size_t)hic * (1u << NB);
+    const size_t off = ((size_t)zb * P.K + j) * Nn + (size_t)hic * (1u << NB);
     uint32_t* row = R + off;
-    const uint2* twj = P.tw + (size_t)j * P.N;
+    const uint2* twj = P.tw + (size_t)j * Nn;
 
     uint32_t v[C::E];
     pdl_trigger();
@@ -395,23 +414,23 @@ __global__ void __launch_bounds__(128, rows_min_blocks(NB, MODE)) k_ntt_rows(Dev
     if constexpr (MODE == ROWS_BOTH) {
         uint32_t a[C::E];
         row_global<NB, 0, true>(a, const_cast<uint32_t*>(RA + off), r, active);
-        row_forward2<NB, 0>(v, a, region, region + REGION_WORDS, rho, r, twj, P.w1, hic, p);
+        row_forward2<NB, 0>(v, a, region, region + REGION_WORDS, rho, r, twj, w1, hic, p);
 #pragma unroll
         for (int e = 0; e < C::E; ++e) v[e] = mont_mul(red_once(red_once(a[e], 2 * p), p), v[e], p, pinv);
-        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p);
+        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, w1, nrows - 1 - hic, p);
         row_global<NB, 0, false>(v, row, r, active);
     } else if constexpr (MODE == ROWS_FUSED) {
-        row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p);
+        row_forward<NB, 0>(v, region, rho, r, twj, w1, hic, p);
         uint32_t a[C::E];
         const size_t za = ra_sel ? (size_t)__ldg(ra_sel + zb) : (size_t)zb;
-        const size_t offa = (za * P.K + j) * P.N + (size_t)hic * (1u << NB);
+        const size_t offa = (za * P.K + j) * Nn + (size_t)hic * (1u << NB);
         row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), true>(a, const_cast<uint32_t*>(RA + offa), r, active);
 #pragma unroll
         for (int e = 0; e < C::E; ++e) v[e] = mont_mul(red_once(red_once(a[e], 2 * p), p), v[e], p, pinv);
-        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, P.w1, P.nrows - 1 - hic, p);
+        row_inverse<NB, C::NPH - 1>(v, region, rho, r, twj, w1, nrows - 1 - hic, p);
         row_global<NB, 0, false>(v, row, r, active);
     } else {
-        row_forward<NB, 0>(v, region, rho, r, twj, P.w1, hic, p);
+        row_forward<NB, 0>(v, region, rho, r, twj, w1, hic, p);
         row_global<NB, (C::NPH > 0 ? C::NPH - 1 : 0), false>(v, row, r, active);
     }
 }
@@ -497,6 +516,7 @@ __device__ __forceinline__ void col_phases(uint32_t* tile, const Tw2* tws, uint3
 // instructions of the one-column form.  GL >= 0: log2 of the row pitch ncols at compile time, so
 // that an element's global address is its group's base plus an immediate.
 constexpr int COL2_TC = 64;
+
 template <int NB, bool INV, int K, int GL>
 __device__ __forceinline__ void col2_phase(uint32_t* tile, const Tw2* tws, uint32_t* gbase, uint32_t ncols_rt,
                                            uint32_t p) {
@@ -634,13 +654,27 @@ void launch_cols_nb(bool inv, dim3 grid, size_t smem, cudaStream_t s, const DevP
     if (e != cudaSuccess) throw_cuda(e, inv ? "launch k_ntt_cols<inverse>" : "launch k_ntt_cols<forward>");
 }
 
+// the row kernel of a mode for line length 2^NB and the plan's w1: a compile-time w1 for the
+// splits of N = 4096 .. 65536 that the batches and the engine use, else w1 from the plan
+template <int NB, int MODE>
+auto row_kernel(int w1) {
+    if constexpr (POLYMULT_ROW_STATIC && NB >= 6 && NB <= 8) {
+        if (w1 == NB) return k_ntt_rows<NB, MODE, NB>;
+        if (w1 == NB - 1) return k_ntt_rows<NB, MODE, NB - 1>;
+    }
+    (void)w1;
+    return k_ntt_rows<NB, MODE, -1>;
+}
+
 template <int NB>
 void launch_rows_nb(int mode, dim3 grid, cudaStream_t s, const DevPlan& P, uint32_t* R, const uint32_t* RA,
                     const uint32_t* ra_sel, bool pdl) {
-    const cudaError_t e = launch_kernel(mode == ROWS_BOTH    ? k_ntt_rows<NB, ROWS_BOTH>
-                                        : mode == ROWS_FUSED ? k_ntt_rows<NB, ROWS_FUSED>
-                                                             : k_ntt_rows<NB, ROWS_FWD>,
-                                        grid, dim3(128), 0, s, pdl, P, R, RA, ra_sel);
+    // grid comes as (row blocks, primes, batch); the static form takes it as (batch, row blocks, primes)
+    const dim3 g = POLYMULT_ROW_STATIC ? dim3(grid.z, grid.x, grid.y) : grid;
+    const cudaError_t e = launch_kernel(mode == ROWS_BOTH    ? row_kernel<NB, ROWS_BOTH>(P.w1)
+                                        : mode == ROWS_FUSED ? row_kernel<NB, ROWS_FUSED>(P.w1)
+                                                             : row_kernel<NB, ROWS_FWD>(P.w1),
+                                        g, dim3(128), 0, s, pdl, P, R, RA, ra_sel);
     if (e != cudaSuccess)
         throw_cuda(e, mode == ROWS_BOTH    ? "launch k_ntt_rows<both operands>"
                       : mode == ROWS_FUSED ? "launch k_ntt_rows<fused>"
@@ -715,8 +749,8 @@ struct ColProbeF {
 template <int NB>
 struct RowProbeF {
     static void run() {
-        const void* fns[3] = {(const void*)k_ntt_rows<NB, ROWS_FWD>, (const void*)k_ntt_rows<NB, ROWS_FUSED>,
-                              (const void*)k_ntt_rows<NB, ROWS_BOTH>};
+        const void* fns[3] = {(const void*)k_ntt_rows<NB, ROWS_FWD, -1>, (const void*)k_ntt_rows<NB, ROWS_FUSED, -1>,
+                              (const void*)k_ntt_rows<NB, ROWS_BOTH, -1>};
         for (const void* f : fns) {
             cudaFuncAttributes fa{};
             const cudaError_t e = cudaFuncGetAttributes(&fa, f);

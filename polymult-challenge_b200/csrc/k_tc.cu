@@ -82,6 +82,32 @@ __device__ __forceinline__ void umma_u8(uint32_t d_tmem, uint64_t adesc, uint64_
         : "memory");
 }
 
+// D[tmem] (+)= A[tmem] * B[smem]^T, unsigned bytes, s32 accumulate; one thread.  A in tensor
+// memory is K-major: lane m holds row m, and each 32-bit column holds 4 consecutive K bytes.
+__device__ __forceinline__ void umma_u8_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// This warp's 32 TMEM lanes x 8 consecutive 32-bit columns from registers (asynchronous: visible
+// to the tensor core after tmem_wait_st and a before-thread-sync fence).
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// 16-byte asynchronous global -> shared copy, L2 only (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
                  : "memory");
@@ -823,6 +849,273 @@ __global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tc(DevPlan P, const u
     if (warp == 0) tmem_dealloc(tmem, nbuf * AS);
 }
 
+// ----------------------------------------------------------------------------------------
+// CRT with the A operand in tensor memory (points of at most 128 primes and 256 result bytes,
+// column chunks of at least 4 columns).  Persistent, warp-specialised, 512 threads.
+//   producers (warps 0-7, two threads per position m, one per half of the A columns):
+//     * the tile's residues arrive as 16-byte cp.async copies (4 positions of one prime each)
+//       into a staging tile [prime][128 positions] in shared memory -- a quarter of the copy
+//       instructions of per-residue copies, and decoupled from the MMA: the next tile's copies
+//       are issued as soon as this tile's residues have been read out of the staging tile;
+//     * each thread reads its position's residues (already y_j, unreduced in [0, 2p)) and writes
+//       them straight into one of two A buffers in tensor memory with tcgen05.st: a 32-bit TMEM
+//       column of A holds 4 consecutive K bytes, exactly one residue's bytes, so A's column j is
+//       y_j and no byte shuffling is needed; sums y_j / p_j in fp32 meanwhile;
+//     * v = round(sum) goes into column K (the B image's v column holds the bytes of T_1);
+//     * thread 0 issues the MMAs (A from TMEM buffer i & 1, B from shared memory) into the one
+//       accumulator once the epilogue has read the previous tile's, and commits to mma_done[i & 1].
+//   epilogue (warps 8-15): as in k_crt_tc -- accumulator bytes -> limbs, fold, -q, coalesced
+//     stores -- releasing the accumulator (acc_empty) as soon as its TMEM reads are done.
+// TMEM: accumulator in columns [0, 256), A buffers at 256 and 384 (ncolA <= 128 columns each).
+// smem: [B image][staging KP x 128 words][z 128 x zs][1/p x KP][partial sums 2 x 128]
+//       [bars: B, mma_done 2, acc_empty][slot][abort]
+// ----------------------------------------------------------------------------------------
+namespace {
+constexpr uint32_t TM_ACOL = 256;  // first A buffer's TMEM column (the second at +128)
+
+struct CrtTmSmem {
+    unsigned char* b;
+    uint32_t* stg;
+    uint32_t* z;
+    float* rcp;
+    float* spart;
+    uint64_t* bars;
+    uint32_t* slot;
+    volatile int* abort;
+};
+
+__host__ __device__ inline size_t crt_tm_stg_words(const DevPlan& P) { return (size_t)P.KP * TC_M; }
+
+__device__ __forceinline__ CrtTmSmem crt_tm_smem(unsigned char* base, const DevPlan& P) {
+    CrtTmSmem m;
+    m.b = base;
+    m.stg = reinterpret_cast<uint32_t*>(m.b + (size_t)P.crt_nrows * P.crt_kbytes);
+    m.z = m.stg + crt_tm_stg_words(P);
+    m.rcp = reinterpret_cast<float*>(m.z + (size_t)TC_M * crt_zstride(P.L));
+    m.spart = m.rcp + P.KP;
+    m.bars = reinterpret_cast<uint64_t*>(m.spart + 2 * TC_M);
+    m.slot = reinterpret_cast<uint32_t*>(m.bars + 4);
+    m.abort = reinterpret_cast<volatile int*>(m.slot + 1);
+    return m;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(CRT_TC_THREADS, 1) k_crt_tm(DevPlan P, const uint32_t* __restrict__ R, ChunkMap C,
+                                                              uint32_t npos, uint32_t nbatch,
+                                                              uint32_t* __restrict__ out) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const CrtTmSmem S = crt_tm_smem(smem_raw, P);
+    uint64_t *bar_b = S.bars, *mma_done = S.bars + 1, *acc_empty = S.bars + 3;
+    const int K = P.K, KP = P.KP, L = P.L, kb = P.crt_kbytes, nrows_b = P.crt_nrows;
+    const int ncolA = kb / 4;                 // A columns (multiple of 8, <= 128): primes, v, padding
+    const int nblk = ncolA / 8, nb0 = (nblk + 1) / 2;  // 8-column blocks; half 0 owns blocks [0, nb0)
+    const int vblk = K / 8;                   // the block holding v's column K
+    const int zl = crt_zl(L), zs = crt_zstride(L);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t tiles_per_batch = (npos + TC_M - 1) / TC_M;
+    const uint32_t ntiles = tiles_per_batch * nbatch;
+    const size_t N = P.N;
+
+    if (threadIdx.x == 0) {
+        mbar_init(bar_b, 1);
+        mbar_init(mma_done, 1);
+        mbar_init(mma_done + 1, 1);
+        mbar_init(acc_empty, CRT_EPI_THREADS);
+        *S.abort = 0;
+        bulk_g2s_all(S.b, P.crt_b, (uint32_t)((size_t)nrows_b * kb), bar_b);
+    }
+    for (int j = threadIdx.x; j < KP; j += blockDim.x) S.rcp[j] = P.rcp[j];
+    if (warp == 0) tmem_alloc(S.slot, 512);
+    pdl_wait();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    pdl_trigger();  // after this block's TMEM allocation
+    const uint32_t tmem = *S.slot;
+    uint32_t issued = 0;   // thread 0: tiles whose MMAs it committed
+    bool b_seen = false;   // thread 0: the B image has landed
+
+    // the 16-byte copies of a tile's residues into the staging tile: copy q = (prime j, group c4
+    // of 4 positions); groups past the tile's last position re-read the tile's first group
+    auto issue_copies = [&](uint32_t tile) {
+        const uint32_t bt = tile / tiles_per_batch;
+        const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
+        const uint32_t* rb = R + (size_t)bt * P.Kr * N;
+        for (int q = threadIdx.x; q < K * (TC_M / 4); q += CRT_PROD_THREADS) {
+            const int j = q / (TC_M / 4), c4 = q - j * (TC_M / 4);
+            const uint32_t pos = pos0 + 4u * (uint32_t)c4 < npos ? pos0 + 4u * (uint32_t)c4 : pos0;
+            cp_async16(S.stg + (size_t)j * TC_M + 4 * c4, rb + (size_t)j * N + chunk_pos_to_n(P, C, pos));
+        }
+    };
+
+    if (threadIdx.x < CRT_PROD_THREADS) {
+        // ---------------- producers ----------------
+        const int m = threadIdx.x & (TC_M - 1), h = threadIdx.x >> 7;
+        const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+        const int blk0 = h ? nb0 : 0, blk1 = h ? nblk : nb0;
+        uint32_t i = 0;
+        if (blockIdx.x < ntiles) issue_copies(blockIdx.x);
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            if (named_sync_or(1, CRT_PROD_THREADS, *S.abort != 0)) break;
+            const int b = (int)(i & 1);
+            const uint32_t bt = tile / tiles_per_batch;
+            const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
+            cp_async_wait_all();
+            named_sync(1, CRT_PROD_THREADS);  // every copy of the tile has landed
+            // A buffer b was last read by tile i - 2's MMAs
+            if (i >= 2) wait_or_abort(mma_done + b, ((i - 2) >> 1) & 1, S.abort, P.wait_clocks);
+            tc_fence_after();
+            const uint32_t acol = tmem + lane_base + TM_ACOL + 128u * (uint32_t)b;
+            float s = 0.f;
+            for (int blk = blk0; blk < blk1; ++blk) {
+                if (blk == vblk) continue;  // written with v below
+                uint32_t r[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const int j = 8 * blk + c;
+                    const uint32_t y = j < K ? S.stg[(size_t)j * TC_M + m] : 0u;
+                    r[c] = y;
+                    s = fmaf((float)y, j < KP ? S.rcp[j] : 0.f, s);
+                }
+                tmem_st8(acol + 8u * (uint32_t)blk, r);
+            }
+            // the v block's primes (before column K)
+            uint32_t rv[8];
+            const bool own_v = vblk >= blk0 && vblk < blk1;
+            if (own_v) {
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const int j = 8 * vblk + c;
+                    const uint32_t y = j < K ? S.stg[(size_t)j * TC_M + m] : 0u;
+                    rv[c] = y;
+                    s = fmaf((float)y, j < K ? S.rcp[j] : 0.f, s);
+                }
+            }
+            S.spart[h * TC_M + m] = s;
+            named_sync(1, CRT_PROD_THREADS);  // staging read out, both halves' sums visible
+            const uint32_t nxt = tile + gridDim.x;
+            if (nxt < ntiles) issue_copies(nxt);  // overlaps this tile's MMAs and epilogue
+            if (own_v) {
+                // v = round(sum y'_j / p_j): |x| < M/8 keeps the sum within 1/8 of an integer, further
+                // than 1/4 is a failed check; the residues' multiples of p_j make v' <= 2K - 1 < 256
+                const float sum = S.spart[m] + S.spart[TC_M + m];
+                const float vf = rintf(sum);
+                if ((uint32_t)m < npos - pos0 && fabsf(sum - vf) > 0.25f) flag_error(P.status, DEV_ERR_CRT_BOUND);
+                rv[K - 8 * vblk] = (uint32_t)min(max((int)vf, 0), 2 * K - 1);
+                tmem_st8(acol + 8u * (uint32_t)vblk, rv);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            named_sync(1, CRT_PROD_THREADS);  // A buffer b complete
+            if (threadIdx.x == 0) {
+                bool ok = *S.abort == 0;
+                if (ok && !b_seen) ok = b_seen = wait_or_abort(bar_b, 0, S.abort, P.wait_clocks);
+                // the single accumulator: tile i - 1's epilogue must have read it
+                if (ok && i > 0) ok = wait_or_abort(acc_empty, (i - 1) & 1, S.abort, P.wait_clocks);
+                if (ok) {
+                    tc_fence_after();
+                    const uint32_t sbo = 8u * (uint32_t)kb;
+                    const uint32_t idesc = idesc_u8(nrows_b);
+                    const uint32_t a_tm = tmem + TM_ACOL + 128u * (uint32_t)b;
+                    for (int kk = 0; kk < kb / 32; ++kk) {
+                        const uint64_t bd = sdesc(smem_addr(S.b) + 256u * kk, 128u, sbo);
+                        umma_u8_ts(tmem, a_tm + 8u * (uint32_t)kk, bd, idesc, kk > 0 ? 1u : 0u);
+                    }
+                    umma_commit(mma_done + b);
+                    ++issued;
+                }
+            }
+        }
+        cp_async_wait_all();  // no copy of this thread may still be in flight at exit
+    } else {
+        // ---------------- epilogue ----------------
+        const int et = threadIdx.x - CRT_PROD_THREADS;
+        const int hf = et >> 7, m = (warp & 3) * 32 + lane;
+        const int nl = nrows_b / 4;
+        const int lh = ((nl + 1) / 2 + 3) / 4 * 4;
+        uint32_t* z = S.z + (size_t)m * zs;
+        uint32_t i = 0;
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            if (named_sync_or(2, CRT_EPI_THREADS, *S.abort != 0)) break;
+            const uint32_t bt = tile / tiles_per_batch;
+            const uint32_t pos0 = (tile - bt * tiles_per_batch) * TC_M;
+            const int cnt = (int)min((uint32_t)TC_M, npos - pos0);
+            const bool valid = m < cnt;
+            const bool got =
+                __all_sync(0xffffffffu, wait_or_abort(mma_done + (i & 1), (i >> 1) & 1, S.abort, P.wait_clocks));
+            tc_fence_after();
+            const uint32_t tacc = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+            uint64_t carry = 0;
+            const int c0 = hf ? lh / 4 : 0, c1 = hf ? nl / 4 : lh / 4;
+            int l = 4 * c0;
+            for (int c16 = c0; c16 < c1; c16 += 2) {
+                uint32_t r[2][16];
+                const bool two = c16 + 1 < c1;
+                if (got) {
+                    tmem_ld16_async(tacc + (uint32_t)(16 * c16), r[0]);
+                    if (two) tmem_ld16_async(tacc + (uint32_t)(16 * (c16 + 1)), r[1]);
+                    tmem_wait_ld();
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) r[0][k] = r[1][k] = 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    if (u == 1 && !two) break;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q, ++l) {
+                        const uint64_t lo = (uint64_t)r[u][4 * q] + (uint64_t)r[u][4 * q + 1] * 256u;
+                        const uint64_t hi = (uint64_t)r[u][4 * q + 2] + (uint64_t)r[u][4 * q + 3] * 256u;
+                        const uint64_t t = carry + lo + (hi << 16);
+                        if (l < zl) z[l] = (uint32_t)t;
+                        carry = t >> 32;
+                    }
+                }
+            }
+            if (hf) {
+                for (; l < zl; ++l) {
+                    z[l] = (uint32_t)carry;
+                    carry >>= 32;
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(acc_empty);  // the accumulator is free for the next tile's MMAs
+            named_sync(2, CRT_EPI_THREADS);
+            if (hf == 0 && valid) {
+                for (int k = lh; carry && k < zl; ++k) {  // half 0's carry-out into half 1's limbs
+                    const uint64_t t = (uint64_t)z[k] + carry;
+                    z[k] = (uint32_t)t;
+                    carry = t >> 32;
+                }
+                crt_reduce_mod_q(z, zl, P);
+            }
+            named_sync(2, CRT_EPI_THREADS);
+            uint32_t* o = out + ((size_t)bt * npos + pos0) * L;
+            const int tot = cnt * L;
+            const int qL = CRT_EPI_THREADS / L, rL = CRT_EPI_THREADS - qL * L;
+            int mm = et / L, col = et - mm * L;
+            for (int w = et; w < tot; w += CRT_EPI_THREADS) {
+                o[w] = S.z[(size_t)mm * zs + col];
+                mm += qL;
+                col += rL;
+                if (col >= L) {
+                    col -= L;
+                    ++mm;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (*S.abort) flag_error(P.status, DEV_ERR_WAIT);
+        // copies and MMAs still in flight must land before this CTA's memory goes away
+        if (!b_seen) mbar_wait_bounded(bar_b, 0, P.wait_clocks);
+        if (issued) mbar_wait_bounded(mma_done + ((issued - 1) & 1), ((issued - 1) >> 1) & 1, P.wait_clocks);
+    }
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
 // Self-test of the bounded waits (pm_selftest_wait): one block waits on an mbarrier that nothing
 // arrives on -- thread 0 with mbar_wait_bounded, warp 1 with wait_or_abort, whose first lane to
 // time out raises the shared abort flag for the others -- and must give up after `limit` clocks
@@ -850,6 +1143,11 @@ __global__ void __launch_bounds__(64) k_wait_selftest(uint32_t* status, long lon
 size_t rns_tc_smem(const DevPlan& P, int ring) {
     return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + (size_t)ring * TC_M * P.L * 4 + 7 * 8 + 8 +
            (size_t)P.KP * 8;
+}
+
+size_t crt_tm_smem(const DevPlan& P) {
+    return (size_t)P.crt_nrows * P.crt_kbytes + crt_tm_stg_words(P) * 4 + (size_t)TC_M * crt_zstride(P.L) * 4 +
+           (size_t)P.KP * 4 + 2 * TC_M * 4 + 4 * 8 + 16;
 }
 
 size_t crt_tc_smem(const DevPlan& P, bool partial) {

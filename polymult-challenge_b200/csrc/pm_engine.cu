@@ -23,6 +23,11 @@
 
 #include "pm_kernels.cuh"
 
+// POLYMULT_CRT_TM: the single-tile CRT runs k_crt_tm (A operand in tensor memory) where it applies
+#ifndef POLYMULT_CRT_TM
+#define POLYMULT_CRT_TM 1
+#endif
+
 #if defined(__x86_64__)
 #include <immintrin.h>
 #endif
@@ -192,6 +197,9 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
             for (const DecBlock& b : dec_blocks_) smem_dec_ = std::max(smem_dec_, b.smem);
         }
         if (crt_tc_) smem_crt_ = crt_tc_smem(dp_);
+        // the single-tile CRT with its A operand in tensor memory where it applies (POLYMULT_CRT_TM)
+        crt_tm_ = POLYMULT_CRT_TM && crt_tc_ && plan_.KP <= 128 && dp_.crt_nrows <= 256 &&
+                  dp_.crt_kbytes <= 512 && crt_tm_smem(dp_) <= smem_optin_;
         // multiplies per launch group of run_device: up to POLYMULT_GROUP_WORDS residue words
         // per operand (default 64 Mi: 8 multiplies at N = 65536, W = 1747, 512 MB of residue
         // scratch), at most 256.  Measured there: 1 multiply per group 4083 mults/s, 2 4789,
@@ -326,7 +334,8 @@ void Engine::setup_launch_shapes() {
     const Probe probes[] = {{(const void*)k_rns_plain, "k_rns_plain"},
                             {(const void*)k_crt_plain, "k_crt_plain"},
                             {(const void*)k_rns_tc, "k_rns_tc"},
-                            {(const void*)k_crt_tc, "k_crt_tc"}};
+                            {(const void*)k_crt_tc, "k_crt_tc"},
+                            {(const void*)k_crt_tm, "k_crt_tm"}};
     for (const Probe& pr : probes) {
         cudaFuncAttributes fa{};
         cuda_check(cudaFuncGetAttributes(&fa, pr.fn), (std::string("kernel image ") + pr.name).c_str());
@@ -336,6 +345,7 @@ void Engine::setup_launch_shapes() {
     cuda_check(cudaFuncSetAttribute(k_crt_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_rns_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_crt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
+    cuda_check(cudaFuncSetAttribute(k_crt_tm, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
     cuda_check(cudaFuncSetAttribute(k_crt_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, mx), "smem attr");
 }
 
@@ -802,7 +812,13 @@ void Engine::launch_rows_both(uint32_t* R, const uint32_t* RA, uint32_t nb, cuda
 void Engine::launch_crt(const uint32_t* R, Chunk ch, uint32_t nb, uint32_t* out, cudaStream_t s, size_t poff,
                         bool pdl) const {
     const uint32_t npos = plan_.nrows * ch.cw;
-    if (crt_tc_) {
+    if (crt_tm_ && ch.cw >= 4 && ch.col0 % 4 == 0) {
+        const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
+        const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
+        cuda_check(launch_kernel(k_crt_tm, dim3(grid), dim3(CRT_TC_THREADS), crt_tm_smem(dp_), s, pdl, dp_, R,
+                                 chunk_map(ch), npos, nb, out),
+                   "launch k_crt_tm");
+    } else if (crt_tc_) {
         const uint32_t tiles = (npos + TC_M - 1) / TC_M * nb;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms_);
         const CrtPartial full{nullptr, nullptr, CRT_FULL, 0, 0};

@@ -169,6 +169,7 @@ class Engine {
     int device_ = 0;
     int form_ = GEMM_PLAIN;
     bool dec_tc_ = false, crt_tc_ = false;  // which contractions run on the tensor cores
+    bool crt_tm_ = false;                   // the single-tile CRT takes k_crt_tm (A in tensor memory)
     bool crt_blocked_ = false;              // the tensor-core CRT runs in blocks (K > one tile)
     std::vector<DecBlock> dec_blocks_;
     std::vector<CrtBlock> crt_blocks_;

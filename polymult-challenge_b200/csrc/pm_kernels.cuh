@@ -79,6 +79,10 @@ struct CrtPartial {
 __global__ void k_crt_tc(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out,
                          CrtPartial part, CrtPrimeBlocks pbs);
 __global__ void k_crt_finish(DevPlan P, const uint32_t* zp, const float* sp, uint32_t total, uint32_t* out);
+// The single-tile CRT with its A operand in tensor memory (k_tc.cu): points with KP <= 128 and
+// crt_nrows <= 256, column chunks of at least 4 columns starting on a multiple of 4.
+__global__ void k_crt_tm(DevPlan P, const uint32_t* R, ChunkMap C, uint32_t npos, uint32_t nbatch, uint32_t* out);
+size_t crt_tm_smem(const DevPlan& P);
 // 64-bit digests of `count` arrays of `words` words (k_digest.cu): out_dev[count] (device) is
 // cleared and filled on stream s; digest_host computes the same value on the host
 void launch_digest(const uint32_t* x, uint64_t words, uint32_t count, uint64_t* out_dev, cudaStream_t s);
