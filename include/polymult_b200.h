@@ -249,7 +249,8 @@ int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int
  * a task ran other than once or was still running when the set returned.  *failures gets that
  * count (0 expected).  `vary` bit 0: task counts 1..64 instead of 64 every time; bit 1: workers
  * park between task sets (20 us idle limit, a 300 us pause before every third set) so that each
- * set has to wake them.  No GPU needed. */
+ * set has to wake them; bit 2: every other set is opened without the caller (the pipeline's
+ * asynchronous staging) and joined after some work of the caller.  No GPU needed. */
 int pm_selftest_host_pool(uint32_t pools, uint32_t runs, uint32_t workers, int vary, uint64_t* failures);
 
 /* Test hook, host-only: after `skip` more residue-scratch allocations of any context (each

@@ -313,7 +313,8 @@ const char* pm_last_error(void) { return g_last_error.c_str(); }
 int pm_selftest_host_pool(uint32_t pools, uint32_t runs, uint32_t workers, int vary, uint64_t* failures) {
     if (!failures || workers > 63) return fail(PM_ERR_INVALID, "bad self-test arguments");
     return guarded(
-        [&] { *failures = pm::host_pool_selftest(pools, runs, (int)workers, (vary & 1) != 0, (vary & 2) != 0); });
+        [&] { *failures = pm::host_pool_selftest(pools, runs, (int)workers, (vary & 1) != 0, (vary & 2) != 0,
+                                                     (vary & 4) != 0); });
 }
 
 int pm_plan_selfcheck(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int32_t* K_out) {

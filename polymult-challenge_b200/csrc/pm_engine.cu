@@ -527,7 +527,8 @@ void Engine::setup_host_pipeline() {
     set_chunk_schedule(std::min<uint32_t>(body, plan_.ncols), std::min<uint32_t>(body, plan_.ncols), 0);
     set_chunk_schedule(std::min<uint32_t>(body, plan_.ncols), std::min<uint32_t>(body, plan_.ncols), 1);
     cuda_check(cudaEventCreateWithFlags(&ev_fused_, cudaEventDisableTiming), "event");
-    // 8 copying threads (7 workers + the caller) by default.  On the 16-CPU B200 hosts measured,
+    // 7 workers by default: they copy while the caller issues a chunk's CUDA calls, and the caller
+    // joins them once it is done (8 copying threads at most).  On the 16-CPU B200 hosts measured,
     // 12 threads stage an operand pair faster in isolation (0.63 ms against 1.0 ms) but made the
     // end-to-end call slower and far more variable inside a full process (p50 1.51 ms, p99 5.6 ms
     // against 1.13 / 1.2 ms): spinning workers then compete with the process's other threads.
@@ -1005,20 +1006,11 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     ensure_scratch(1);
     const uint32_t nrows = plan_.nrows, ncols = plan_.ncols, L = plan_.L;
     const uint32_t* src[2] = {a, b};
-    // staging tasks of at least 128 KB of the chunk each (up to 64, one per row at most): a small
-    // chunk is copied by the calling thread alone rather than handed to the pool
+    // copy jobs of one column chunk: tasks of at least 64 KB of the chunk each (up to 64, one
+    // row at most), taken from the pool's word by whichever thread is free
     auto tasks_for = [&](uint32_t cw) {
         const size_t bytes = (size_t)nrows * cw * L * 4;
-        return (uint32_t)std::max<size_t>(1, std::min<size_t>({(size_t)nrows, 64, bytes >> 17}));
-    };
-    auto staged_copy = [&](uint32_t cw, const std::function<void(uint32_t)>& row_copy) {
-        const uint32_t nt = tasks_for(cw), rpt = (nrows + nt - 1) / nt;
-        auto task = [&](int t) {
-            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
-            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r) row_copy(r);
-        };
-        if (nt == 1) task(0);
-        else pool_->run((int)nt, task);
+        return (uint32_t)std::max<size_t>(1, std::min<size_t>({(size_t)nrows, 64, bytes >> 16}));
     };
     // operands already in page-locked memory skip the host staging: each column chunk moves
     // with one strided DMA copy (rows of cw * L words at a pitch of ncols * L words); with all
@@ -1028,6 +1020,7 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     const bool direct_out = host_range_pinned(c, opbytes);
     const int kind = direct_in[0] && direct_in[1] && direct_out ? 1 : 0;
     const std::vector<Chunk>& cout = cout_[kind];
+    const size_t nout = cout.size();
     // input items (operand, column chunk): both operands in the schedule's input chunks; with
     // direct copies a moves in one piece (each copy costs a few microseconds of DMA set-up, and
     // a's transform is hidden under b's transfer anyway) and only b is chunked
@@ -1039,16 +1032,46 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     for (const Chunk& ch : cin_[kind]) items.push_back({1, ch});
     const int nin = (int)items.size();
 
-    // gather input item i into pinned memory, layout [row][col-in-chunk][limb]
-    auto stage = [&](int i) {
+    // The pool's open copy job.  The workers copy chunk i + 1 (or scatter output chunk oc)
+    // while this thread issues chunk i's copies and kernels (12-20 us of API calls per chunk),
+    // then joins in with wait(); the guard, declared after the job, waits for it before the
+    // job goes out of scope if anything below throws.
+    std::function<void(int)> job;
+    struct JoinPool {
+        HostPool* p;
+        ~JoinPool() { p->wait(); }
+    } join_pool{pool_.get()};
+    const bool ntg = nt_gather_;
+    // opens the staging job of input item i: layout [row][col-in-chunk][limb] in pinned memory
+    // (nothing to do for an operand already page-locked)
+    auto stage_start = [&](int i) {
         const int P = items[i].first;
-        if (direct_in[P]) return;
+        if (direct_in[P]) return false;
         const Chunk ch = items[i].second;
         uint32_t* dst = h_in_[P] + (size_t)ch.col0 * nrows * L;
+        const uint32_t* s = src[P];
         const size_t seg = (size_t)ch.cw * L;
-        staged_copy(ch.cw, [&](uint32_t r) {
-            stream_copy(dst + r * seg, src[P] + ((size_t)r * ncols + ch.col0) * L, seg * 4, nt_gather_);
-        });
+        const uint32_t nt = tasks_for(ch.cw), rpt = (nrows + nt - 1) / nt;
+        job = [=](int t) {
+            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
+            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r)
+                stream_copy(dst + r * seg, s + ((size_t)r * ncols + ch.col0) * L, seg * 4, ntg);
+        };
+        pool_->start((int)nt, job);
+        return true;
+    };
+    // opens the job that scatters output chunk oc from pinned memory into c
+    auto scatter_start = [&](size_t oc) {
+        const Chunk ch = cout[oc];
+        const uint32_t* srcc = h_out_ + (size_t)ch.col0 * nrows * L;
+        const size_t seg = (size_t)ch.cw * L;
+        const uint32_t nt = tasks_for(ch.cw), rpt = (nrows + nt - 1) / nt;
+        job = [=](int t) {
+            const uint32_t r1 = std::min<uint32_t>(nrows, (uint32_t)(t + 1) * rpt);
+            for (uint32_t r = (uint32_t)t * rpt; r < r1; ++r)
+                stream_copy(c + ((size_t)r * ncols + ch.col0) * L, srcc + r * seg, seg * 4);
+        };
+        pool_->start((int)nt, job);
     };
     uint32_t* dR[2] = {d_ra_, d_rb_};
     using clk = std::chrono::steady_clock;
@@ -1058,18 +1081,21 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     // POLYMULT_PROFILE: device timeline from timing events on the pipeline's streams
     std::vector<std::pair<std::string, cudaEvent_t>> marks;
     std::vector<double> staged_us;  // host time each input chunk finished staging
+    std::vector<double> issued_us;  // host time each input chunk's copies and kernels were issued
     auto mark = [&](const std::string& name, cudaStream_t st) {
         if (!profile_ || marks.size() >= trace_ev_.size()) return;
         cuda_check(cudaEventRecord(trace_ev_[marks.size()], st), "record");
         marks.emplace_back(name, trace_ev_[marks.size()]);
     };
     mark("start", s_h2d_);
-    stage(0);
+    if (stage_start(0)) pool_->wait();
     t_stage0 = clk::now();
     for (int i = 0; i < nin; ++i) {
         const int P = items[i].first;
         const Chunk ch = items[i].second;
         const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
+        // the next chunk is copied by the workers while this thread issues this one
+        const bool staging = i + 1 < nin && stage_start(i + 1);
         // the last input chunk runs on stream 0, after a's row pass and b's other chunks, so
         // that its kernels, the fused row pass and the first output chunk's follow each other
         // in one stream (each launch overlapping the previous kernel's tail)
@@ -1098,17 +1124,16 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
             launch_rows(false, d_ra_, nullptr, 1, s_comp_[0]);
             mark("rowA", s_comp_[0]);
         }
-        if (i + 1 < nin) {
-            stage(i + 1);
-            if (profile_) staged_us.push_back(us(clk::now()));
-        }
+        if (profile_ && i + 1 < nin) issued_us.push_back(us(clk::now()));
+        if (staging) pool_->wait();
+        if (profile_ && i + 1 < nin) staged_us.push_back(us(clk::now()));
     }
     // stream 0 has run a's row pass and b's last chunk after the others
     cudaStream_t s0 = s_comp_[0];
     launch_rows(true, d_rb_, d_ra_, 1, s0, nullptr, true);
     if (kind == 0) cuda_check(cudaEventRecord(ev_fused_, s0), "record");
     mark("fused", s0);
-    for (size_t oc = 0; oc < cout.size(); ++oc) {
+    auto issue_out = [&](size_t oc) {
         const Chunk ch = cout[oc];
         const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
         // staged calls spread the output chunks over three streams; direct-copy calls run them
@@ -1132,25 +1157,34 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
                        "D2H");
         cuda_check(cudaEventRecord(ev_out_[oc], s_d2h_), "record");
         mark("d2h" + std::to_string(oc), s_d2h_);
-    }
-    // device status word -> pinned memory behind the last D2H (s_d2h has waited on every CRT)
-    cuda_check(cudaMemcpyAsync(h_status_, dp_.status, 4, cudaMemcpyDeviceToHost, s_d2h_), "status D2H");
-    cuda_check(cudaMemsetAsync(dp_.status, 0, 4, s_d2h_), "status clear");
-    cuda_check(cudaEventRecord(ev_out_[cout.size() - 1], s_d2h_), "record");  // re-recorded: the host waits on it
+        if (oc + 1 == nout) {
+            // device status word -> pinned memory behind the last D2H (s_d2h has waited on every CRT)
+            cuda_check(cudaMemcpyAsync(h_status_, dp_.status, 4, cudaMemcpyDeviceToHost, s_d2h_), "status D2H");
+            cuda_check(cudaMemsetAsync(dp_.status, 0, 4, s_d2h_), "status clear");
+            cuda_check(cudaEventRecord(ev_out_[oc], s_d2h_), "record");  // re-recorded: the host waits on it
+        }
+    };
+    // Output chunks issued before the host waits on the first: all of them when nothing is
+    // scattered on the host; else the first three (one per compute stream), then more for as
+    // long as the first D2H has not finished (the host usually waits here for the device's
+    // last input chunk), and the rest two at a time while the workers scatter earlier ones.
+    // The first scatter is then not held up behind the API calls of every output chunk, and
+    // the device stays ahead of the scatter.
+    size_t issued = direct_out ? nout : std::min<size_t>(3, nout);
+    for (size_t oc = 0; oc < issued; ++oc) issue_out(oc);
+    while (issued < nout && cudaEventQuery(ev_out_[0]) == cudaErrorNotReady) issue_out(issued++);
+    if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();  // the query's answer, not a failure
     cuda_check(cudaGetLastError(), "kernel launch");
     t_inputs = clk::now();
-    for (size_t oc = 0; oc < cout.size(); ++oc) {
+    for (size_t oc = 0; oc < nout; ++oc) {
         cuda_check(cudaEventSynchronize(ev_out_[oc]), "D2H chunk");
         if (oc == 0) t_first_out = clk::now();
-        if (oc + 1 == cout.size()) t_last_out = clk::now();
-        if (direct_out) continue;
-        const Chunk ch = cout[oc];
-        const uint32_t* srcc = h_out_ + (size_t)ch.col0 * nrows * L;
-        const size_t seg = (size_t)ch.cw * L;
-        staged_copy(ch.cw, [&](uint32_t r) {
-            stream_copy(c + ((size_t)r * ncols + ch.col0) * L, srcc + r * seg, seg * 4);
-        });
+        if (oc + 1 == nout) t_last_out = clk::now();
+        if (!direct_out) scatter_start(oc);
+        for (int k = 0; k < 2 && issued < nout; ++k) issue_out(issued++);
+        pool_->wait();
     }
+    cuda_check(cudaGetLastError(), "kernel launch");
     if (profile_) {
         std::fprintf(stderr,
                      "polymult: host: stage0 %.1f us | inputs issued %.1f | first out %.1f | last out %.1f | done %.1f"
@@ -1167,10 +1201,10 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
             }
         }
         std::fprintf(stderr, "%s\n", line.c_str());
-        std::string st = "polymult: host staging done (us):";
-        for (double t : staged_us) {
-            char buf[32];
-            std::snprintf(buf, sizeof buf, " %.1f", t);
+        std::string st = "polymult: host chunk issued / next chunk staged (us):";
+        for (size_t k = 0; k < staged_us.size(); ++k) {
+            char buf[48];
+            std::snprintf(buf, sizeof buf, " %.1f/%.1f", issued_us[k], staged_us[k]);
             st += buf;
         }
         std::fprintf(stderr, "%s\n", st.c_str());

@@ -58,6 +58,12 @@ bool HostPool::take_one() {
 }
 
 void HostPool::run(int n, const std::function<void(int)>& fn) {
+    start(n, fn);
+    wait();
+}
+
+void HostPool::start(int n, const std::function<void(int)>& fn) {
+    if (open_) throw std::logic_error("HostPool: a job is already open");
     if (n <= 0) return;
     if (n > 0xFFFF) throw std::length_error("HostPool: more than 65535 tasks in one job");
     // The previous job is finished (its run() returned), so no live ticket reads fn_ now; late
@@ -71,9 +77,16 @@ void HostPool::run(int n, const std::function<void(int)>& fn) {
         wake_seq_.fetch_add(1, std::memory_order_seq_cst);
         futex_wake_all(&wake_seq_);
     }
+    open_ = true;
+    open_n_ = (uint32_t)n;
+}
+
+void HostPool::wait() {
+    if (!open_) return;
     while (take_one()) {
     }
-    while (finished_.load(std::memory_order_acquire) < (uint32_t)n) relax();
+    while (finished_.load(std::memory_order_acquire) < open_n_) relax();
+    open_ = false;
 }
 
 void HostPool::worker() {
@@ -98,7 +111,7 @@ void HostPool::worker() {
     }
 }
 
-uint64_t host_pool_selftest(uint32_t pools, uint32_t runs, int workers, bool vary, bool park) {
+uint64_t host_pool_selftest(uint32_t pools, uint32_t runs, int workers, bool vary, bool park, bool split) {
     uint64_t bad = 0;
     std::vector<std::atomic<int>> hits(64);
     for (uint32_t pi = 0; pi < pools; ++pi) {
@@ -115,8 +128,16 @@ uint64_t host_pool_selftest(uint32_t pools, uint32_t runs, int workers, bool var
                 if (t >= 0 && t < 64) hits[t].fetch_add(1);
                 inflight.fetch_sub(1);
             };
-            pool.run(n, fn);
-            bool ok = inflight.load() == 0;
+            if (split && it % 2 == 1) {
+                pool.start(n, fn);
+                // the caller's own work between start() and wait()
+                volatile uint64_t x = it;
+                for (int k = 0; k < 2000; ++k) x = x * 6364136223846793005ull + 1442695040888963407ull;
+                pool.wait();
+            } else {
+                pool.run(n, fn);
+            }
+            bool ok = inflight.load() == 0 && !pool.open();
             for (int t = 0; t < 64 && ok; ++t) ok = hits[t].load() == (t < n ? 1 : 0);
             if (!ok) ++bad;
         }

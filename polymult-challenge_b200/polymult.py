@@ -181,10 +181,11 @@ def _u32(arr, shape=None) -> np.ndarray:
     return a
 
 
-def host_pool_selftest(pools: int, runs: int, workers: int = 7, vary: bool = False, park: bool = False) -> int:
+def host_pool_selftest(pools: int, runs: int, workers: int = 7, vary: bool = False, park: bool = False,
+                       split: bool = False) -> int:
     """Stress test of the host staging pool (pm_selftest_host_pool); returns the failures."""
     f = ctypes.c_uint64()
-    flags = (1 if vary else 0) | (2 if park else 0)
+    flags = (1 if vary else 0) | (2 if park else 0) | (4 if split else 0)
     _check(load().pm_selftest_host_pool(pools, runs, workers, flags, ctypes.byref(f)))
     return f.value
 
