@@ -20,45 +20,19 @@
 // them to an mbarrier; each warp then reads its 32 TMEM lanes (one coefficient per thread)
 // with tcgen05.ld for the epilogue.  Every mbarrier wait is bounded by a clock limit and
 // reports DEV_ERR_WAIT instead of hanging.
+#include "pm_async.cuh"
 #include "pm_crt.cuh"
 #include "pm_kernels.cuh"
 
 namespace pm {
 namespace {
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
 
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, P1;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
 
-// Waits for phase `parity` of `bar`; false once `limit` clocks have passed (the plan's
-// wait_clocks: 2e9, about one second).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > limit) return false;
-    return true;
-}
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_smem_to_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // whole warp
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
@@ -159,13 +133,7 @@ __device__ __forceinline__ void issue_gemm_rows(uint32_t tmem_col, uint32_t a_ba
     }
 }
 
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
 
-// TMA-engine bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16),
-// completing `bytes` transactions on `bar`.
 // 4-byte asynchronous global -> shared copy (no register staging); cp_async_wait_all waits for
 // all of this thread's.
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
@@ -173,12 +141,6 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
 
 // One thread: expect and issue a copy of `bytes` (multiple of 16) in pieces of <= 32 KB.
 __device__ __forceinline__ void bulk_g2s_all(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -189,41 +151,9 @@ __device__ __forceinline__ void bulk_g2s_all(void* dst, const void* src, uint32_
     }
 }
 
-__device__ __forceinline__ void named_sync(int id, int n) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
 
-// Barrier over `n` threads on named barrier `id`; true if any participant passed p = true.
-__device__ __forceinline__ bool named_sync_or(int id, int n, bool p) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred ip, op;\n\t"
-        "setp.ne.u32 ip, %1, 0;\n\t"
-        "barrier.red.or.pred op, %2, %3, ip;\n\t"
-        "selp.u32 %0, 1, 0, op;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)p), "r"(id), "r"(n)
-        : "memory");
-    return r != 0;
-}
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
 
-// Bounded wait that also gives up once another thread has set *abort; sets *abort itself
-// when its own limit of `limit` clocks runs out.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort, long long limit) {
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (*abort) return false;
-        if (clock64() - t0 > limit) {
-            *abort = 1;
-            return false;
-        }
-    }
-    return true;
-}
 
 }  // namespace
 

@@ -47,7 +47,8 @@ struct DevPlan {
     int dec_nrows, dec_kbytes;
     int crt_nrows, crt_kbytes;
     uint32_t* status;         // device status word
-    long long wait_clocks;    // limit of every mbarrier wait of the tcgen05 kernels (2e9 clocks, ~1 s)
+    long long wait_clocks;    // limit of every mbarrier wait of the tcgen05 and TMA kernels (2e9 clocks, ~1 s)
+    int col_tma;              // host-side choice: column passes of 64-column tiles take the TMA kernel
 };
 
 // A chunk of coefficient positions: all rows x `cw` columns starting at `col0`, stored

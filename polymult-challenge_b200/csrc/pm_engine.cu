@@ -287,6 +287,8 @@ void Engine::upload_tables() {
     cuda_check(cudaMemset(st, 0, 4), "memset status");
     d.status = st;
     d.wait_clocks = kWaitClocks;
+    // POLYMULT_COL_TMA=0: the column passes keep the one-tile-per-CTA kernels
+    d.col_tma = !(std::getenv("POLYMULT_COL_TMA") && std::getenv("POLYMULT_COL_TMA")[0] == '0');
 }
 
 void Engine::set_status_for_test(uint32_t bits) {
