@@ -120,10 +120,13 @@ int pm_run_device_static(pm_context* ctx, const uint32_t* d_a, const uint32_t* d
  * tables, allocates the residue scratch once, and captures the whole schedule -- one launch
  * per kernel per class, classes spread over up to 8 streams -- into a CUDA graph;
  * pm_batch_run replays it with one graph launch.  The operand pointers are captured: write
- * new inputs into the same buffers between runs.  With PM_BATCH_TUNE the 4-step split and
- * the GEMM form of each class are chosen by timing the candidates on the class's operands
- * (results cached in $POLYMULT_TUNE_CACHE, default ~/.cache/polymult_b200/tune.txt); the
- * tuning runs write the outputs.  Results are bit-identical whatever the choice. */
+ * new inputs into the same buffers between runs.  With PM_BATCH_TUNE each class's
+ * configuration is chosen by timing the candidates on the class's operands: first the 4-step
+ * split and the GEMM form, then the column-pass kernel (TMA pipeline or one tile per CTA), the
+ * CRT GEMM's A-operand placement (tensor or shared memory) and the number of launch groups the
+ * class runs in (1, 2 or 4; fewer multiplies per group need less scratch).  Results are cached
+ * in $POLYMULT_TUNE_CACHE (default ~/.cache/polymult_b200/tune.txt); the tuning runs write the
+ * outputs.  Results are bit-identical whatever the choice. */
 typedef struct pm_batch pm_batch;
 
 typedef struct pm_batch_class {
@@ -137,7 +140,7 @@ typedef struct pm_batch_class {
 } pm_batch_class;
 
 enum pm_batch_flags {
-    PM_BATCH_TUNE = 1,     /* measure and choose split and GEMM form per class */
+    PM_BATCH_TUNE = 1,     /* measure and choose split, GEMM form, kernel variants and launch groups per class */
     PM_BATCH_NO_GRAPH = 2  /* launch the schedule directly on every run instead of a graph */
 };
 
@@ -153,6 +156,9 @@ typedef struct pm_batch_class_info {
     int32_t K, w1, w2;
     int32_t gemm_form;  /* PM_GEMM_PLAIN or PM_GEMM_TENSOR */
     double tuned_ms;    /* measured ms of the chosen configuration; 0 untuned, -1 from the cache */
+    int32_t col_tma;    /* 1: column passes by the TMA-pipelined kernel (256-row lines), 0: one tile per CTA */
+    int32_t crt_tm;     /* 1: CRT GEMM with its A operand in tensor memory, 0: in shared memory (or plain) */
+    uint32_t launch_groups; /* the class's multiplications run as this many launch groups */
 } pm_batch_class_info;
 
 int pm_batch_init(const pm_batch_class* classes, uint32_t nclasses, int gemm_form, int flags, int device,

@@ -1,5 +1,6 @@
 // pm_batch.cpp -- many multiplications of uneven points (N, W, q) in one CUDA-graph launch,
-// with a measured choice of the 4-step split and the GEMM form per point (the autotuner).
+// with a measured choice of the 4-step split, the GEMM form, the kernel variants and the launch
+// groups per point (the autotuner).
 //
 // The reference has no batch path (it multiplies one pair per fherma_run call,
 // solve.cu:1480-1498, with fixed heuristics for the split and the chunking,
@@ -7,7 +8,8 @@
 // `count` multiplications of it whose operands lie contiguously in device memory -- and:
 //   * every class runs as one launch per kernel covering all of its multiplications
 //     (grid.z / the persistent tile range spans the class's batch), so the 8 kernels of a
-//     class see count x the work of one multiply;
+//     class see count x the work of one multiply -- or as 2 or 4 such launch groups in a row
+//     where the tuner measured that faster;
 //   * classes are spread over a few streams (largest work first, each class to the stream
 //     with the least work so far) so that small classes overlap one another on the GPU;
 //   * the whole schedule -- every class's launches, the fork and join between streams -- is
@@ -17,8 +19,10 @@
 // The autotuner (PM_BATCH_TUNE) times, per class, every split w1 in logN/2 - 1 .. logN/2 + 1
 // that the kernels support and both GEMM forms (where the tensor-core form fits) on the
 // class's own operands, CUDA events around 3 repetitions after a warm-up, and keeps the
-// fastest; results are cached per (N, W, count, device) in a text file
-// ($POLYMULT_TUNE_CACHE, default ~/.cache/polymult_b200/tune.txt).
+// fastest; then, on that engine, the column-pass kernel (TMA pipeline / one tile per CTA), the
+// CRT GEMM's A placement (tensor / shared memory) and 1, 2 or 4 launch groups per class.
+// Results are cached per (N, W, count, device) in a text file ($POLYMULT_TUNE_CACHE, default
+// ~/.cache/polymult_b200/tune.txt).
 #include "pm_batch.h"
 
 #include <algorithm>
@@ -49,28 +53,49 @@ std::string cache_path() {
     return std::string(home ? home : "/tmp") + "/.cache/polymult_b200/tune.txt";
 }
 
-// "N W count device-name-with-underscores gemm w1 ms" per line
-std::map<std::string, std::pair<int, int>> read_cache() {
-    std::map<std::string, std::pair<int, int>> m;
+// The tuner's choice for one class.  col_tma / crt_tm: -1 = the engine's default.
+struct Choice {
+    int gemm = 0, w1 = 0;
+    int col_tma = -1, crt_tm = -1;
+    uint32_t groups = 1;
+};
+
+// "N W count device-name-with-underscores gemm w1 ms [col_tma crt_tm groups]" per line (lines
+// written before the variant fields existed keep the engine's defaults and one launch group)
+std::map<std::string, Choice> read_cache() {
+    std::map<std::string, Choice> m;
     std::ifstream f(cache_path());
     std::string line;
     while (std::getline(f, line)) {
         std::istringstream in(line);
         TuneKey k;
-        int gemm = 0, w1 = 0;
+        Choice c;
         double ms = 0;
-        if (in >> k.N >> k.W >> k.count >> k.dev >> gemm >> w1 >> ms) m[k.str()] = {gemm, w1};
+        if (!(in >> k.N >> k.W >> k.count >> k.dev >> c.gemm >> c.w1 >> ms)) continue;
+        int ct = -1, cm = -1;
+        uint32_t g = 1;
+        if (in >> ct >> cm >> g) {
+            c.col_tma = ct;
+            c.crt_tm = cm;
+            c.groups = std::max<uint32_t>(1, g);
+        }
+        m[k.str()] = c;
     }
     return m;
 }
 
-void append_cache(const TuneKey& k, int gemm, int w1, double ms) {
+void append_cache(const TuneKey& k, const Choice& c, double ms) {
     const std::string p = cache_path();
     for (size_t i = 1; i < p.size(); ++i)
         if (p[i] == '/') mkdir(p.substr(0, i).c_str(), 0755);
     std::ofstream f(p, std::ios::app);
-    if (f) f << k.str() << ' ' << gemm << ' ' << w1 << ' ' << ms << '\n';
+    if (f)
+        f << k.str() << ' ' << c.gemm << ' ' << c.w1 << ' ' << ms << ' ' << c.col_tma << ' ' << c.crt_tm << ' '
+          << c.groups << '\n';
 }
+
+// multiplies per launch group when `count` runs in `groups` launch groups
+uint32_t per_group(uint32_t count, uint32_t groups) { return (count + groups - 1) / std::max<uint32_t>(1, groups); }
 
 std::string device_tag(int device) {
     cudaDeviceProp prop{};
@@ -136,11 +161,13 @@ void Batch::release() {
     for (auto& c : cls_) c.eng.reset();
 }
 
-// Picks (gemm form, split) per class -- from the tuning cache, by measurement, or the
-// defaults -- and builds the class's engine with it.
+// Picks per class -- from the tuning cache, by measurement, or the defaults -- the gemm form
+// and split (first stage: one engine per candidate), then the kernel variants and the number
+// of launch groups (second stage: switched on the chosen engine), and builds the class's
+// engine with them.
 void Batch::choose_configs(int gemm_request) {
     const std::string dev = device_tag(device_);
-    std::map<std::string, std::pair<int, int>> cache;
+    std::map<std::string, Choice> cache;
     if (flags_ & PM_BATCH_TUNE) cache = read_cache();
     // one probe scratch, sized for the largest class, while tuning
     uint32_t* probe = nullptr;
@@ -157,8 +184,12 @@ void Batch::choose_configs(int gemm_request) {
             const TuneKey key{s.N, s.W, s.count, dev};
             auto hit = cache.find(key.str());
             if (hit != cache.end()) {
-                opt.w1 = hit->second.second;
-                c.eng.reset(new Engine(s.N, s.W, s.L, s.q, hit->second.first, device_, opt));
+                const Choice& ch = hit->second;
+                opt.w1 = ch.w1;
+                c.eng.reset(new Engine(s.N, s.W, s.L, s.q, ch.gemm, device_, opt));
+                c.eng->set_variant(ch.col_tma < 0 ? c.eng->col_tma() : ch.col_tma != 0,
+                                   ch.crt_tm < 0 ? c.eng->crt_tm() : ch.crt_tm != 0);
+                c.groups = std::min<uint32_t>(std::max<uint32_t>(1, ch.groups), s.count);
                 c.tuned_ms = -1.0;
                 continue;
             }
@@ -202,9 +233,41 @@ void Batch::choose_configs(int gemm_request) {
                 }
             }
             if (!best_eng) throw Unsupported("no kernel configuration fits this point");
+            // second stage on the chosen engine: column-pass kernel (TMA pipeline or one tile per
+            // CTA), CRT GEMM operand placement (A in tensor or shared memory), and the class in
+            // 1, 2 or 4 launch groups (less scratch, the groups' residues closer to L2 size,
+            // against each kernel's fixed costs spread over fewer multiplies)
+            Engine& e = *best_eng;
+            Choice ch;
+            ch.gemm = best_form;
+            ch.w1 = best_w1;
+            ch.col_tma = e.col_tma() ? 1 : 0;
+            ch.crt_tm = e.crt_tm() ? 1 : 0;
+            std::vector<int> cols{ch.col_tma}, crts{ch.crt_tm};
+            if (e.col_tma_applies()) cols.push_back(1 - ch.col_tma);
+            if (e.crt_tm_applies()) crts.push_back(1 - ch.crt_tm);
+            const size_t words = (size_t)s.count * e.plan().K * e.plan().N;
+            for (uint32_t g : {1u, 2u, 4u}) {
+                if (g > s.count) break;
+                e.reserve((size_t)per_group(s.count, g) * e.plan().N);
+                for (int ct : cols)
+                    for (int cm : crts) {
+                        if (g == 1 && ct == ch.col_tma && cm == ch.crt_tm) continue;  // timed above
+                        e.set_variant(ct != 0, cm != 0);
+                        const double ms = time_class(e, s, probe, probe + words, g);
+                        if (ms < best) {
+                            best = ms;
+                            ch.col_tma = ct;
+                            ch.crt_tm = cm;
+                            ch.groups = g;
+                        }
+                    }
+            }
+            e.set_variant(ch.col_tma != 0, ch.crt_tm != 0);
+            c.groups = ch.groups;
             c.eng = std::move(best_eng);
             c.tuned_ms = best;
-            append_cache(key, best_form, best_w1, best);
+            append_cache(key, ch, best);
         }
     } catch (...) {
         if (probe) cudaFree(probe);
@@ -215,8 +278,21 @@ void Batch::choose_configs(int gemm_request) {
     for (auto& c : cls_) c.eng->throw_if_status();
 }
 
-// Mean time (ms) of one run_group over the class on a scratch stream: 1 warm-up, 3 timed.
-double Batch::time_class(const Engine& e, const pm_batch_class& s, uint32_t* ra, uint32_t* rb) {
+// The class's multiplications as `groups` launch groups, one after another on `st`, each
+// reusing the same residue scratch (sized for one group).
+void Batch::run_class(const Engine& e, const pm_batch_class& s, uint32_t groups, uint32_t* ra, uint32_t* rb,
+                      cudaStream_t st) {
+    const uint32_t per = per_group(s.count, groups);
+    const size_t words = (size_t)e.plan().N * e.plan().L;
+    for (uint32_t i0 = 0; i0 < s.count; i0 += per) {
+        const uint32_t n = std::min(per, s.count - i0);
+        e.run_group(s.d_a + i0 * words, s.d_b + i0 * words, s.d_c + i0 * words, n, ra, rb, st);
+    }
+}
+
+// Mean time (ms) of the class's multiplications in `groups` launch groups on a scratch
+// stream: 1 warm-up, 3 timed.
+double Batch::time_class(const Engine& e, const pm_batch_class& s, uint32_t* ra, uint32_t* rb, uint32_t groups) {
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
@@ -224,9 +300,9 @@ double Batch::time_class(const Engine& e, const pm_batch_class& s, uint32_t* ra,
     try {
         cuda_check(cudaEventCreate(&e0), "event");
         cuda_check(cudaEventCreate(&e1), "event");
-        e.run_group(s.d_a, s.d_b, s.d_c, s.count, ra, rb, st);
+        run_class(e, s, groups, ra, rb, st);
         cuda_check(cudaEventRecord(e0, st), "record");
-        for (int r = 0; r < 3; ++r) e.run_group(s.d_a, s.d_b, s.d_c, s.count, ra, rb, st);
+        for (int r = 0; r < 3; ++r) run_class(e, s, groups, ra, rb, st);
         cuda_check(cudaEventRecord(e1, st), "record");
         cuda_check(cudaEventSynchronize(e1), "sync");
         cuda_check(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
@@ -253,7 +329,7 @@ void Batch::alloc_scratch() {
     };
     std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return work(x) > work(y); });
     const size_t ns = std::max<size_t>(1, std::min<size_t>(kMaxStreams, cls_.size()));
-    for (auto& c : cls_) c.eng->reserve((size_t)c.src.count * c.eng->plan().N);
+    for (auto& c : cls_) c.eng->reserve((size_t)per_group(c.src.count, c.groups) * c.eng->plan().N);
     std::vector<double> load(ns, 0.0);
     std::vector<size_t> need(ns, 0);
     sched_.assign(ns, {});
@@ -263,7 +339,7 @@ void Batch::alloc_scratch() {
         load[s] += work(i);
         sched_[s].push_back(i);
         const Plan& P = cls_[i].eng->plan();
-        need[s] = std::max(need[s], (size_t)cls_[i].src.count * P.K * P.N);
+        need[s] = std::max(need[s], (size_t)per_group(cls_[i].src.count, cls_[i].groups) * P.K * P.N);
     }
     streams_.assign(ns, nullptr);
     scratch_.assign(ns, nullptr);
@@ -282,8 +358,7 @@ void Batch::enqueue(cudaStream_t origin) {
         cuda_check(cudaStreamWaitEvent(streams_[s], fork_, 0), "wait");
         for (size_t i : sched_[s]) {
             const Cls& c = cls_[i];
-            c.eng->run_group(c.src.d_a, c.src.d_b, c.src.d_c, c.src.count, scratch_[s], scratch_[s] + scratch_words_[s],
-                             streams_[s]);
+            run_class(*c.eng, c.src, c.groups, scratch_[s], scratch_[s] + scratch_words_[s], streams_[s]);
         }
         cuda_check(cudaEventRecord(joins_[s], streams_[s]), "record");
         cuda_check(cudaStreamWaitEvent(origin, joins_[s], 0), "wait");
@@ -322,7 +397,7 @@ void Batch::sync() {
 int Batch::kernel_launches() const {
     int n = 0;
     for (const auto& c : cls_)
-        if (c.src.count) n += c.eng->kernel_launches_per_group();
+        if (c.src.count) n += (int)c.groups * c.eng->kernel_launches_per_group();
     return n;
 }
 

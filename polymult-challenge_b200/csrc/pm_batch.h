@@ -27,6 +27,7 @@ class Batch {
     size_t classes() const { return cls_.size(); }
     const Engine& engine(size_t i) const { return *cls_[i].eng; }
     double tuned_ms(size_t i) const { return cls_[i].tuned_ms; }
+    uint32_t launch_groups(size_t i) const { return cls_[i].groups; }
     int kernel_launches() const;
     size_t graph_nodes() const { return graph_nodes_; }
     size_t streams() const { return streams_.size(); }
@@ -44,9 +45,12 @@ class Batch {
         std::vector<uint32_t> q;
         std::unique_ptr<Engine> eng;
         double tuned_ms = 0.0;  // measured time of the chosen configuration (0: not tuned, -1: cached)
+        uint32_t groups = 1;    // launch groups the class's multiplications run in
     };
     void choose_configs(int gemm_request);
-    static double time_class(const Engine& e, const pm_batch_class& s, uint32_t* ra, uint32_t* rb);
+    static void run_class(const Engine& e, const pm_batch_class& s, uint32_t groups, uint32_t* ra, uint32_t* rb,
+                          cudaStream_t st);
+    static double time_class(const Engine& e, const pm_batch_class& s, uint32_t* ra, uint32_t* rb, uint32_t groups = 1);
     void alloc_scratch();
     void enqueue(cudaStream_t origin);
     void capture();

@@ -240,6 +240,9 @@ int pm_batch_get_class(const pm_batch* batch, uint32_t index, pm_batch_class_inf
     out->w2 = e.plan().w2;
     out->gemm_form = e.gemm_form();
     out->tuned_ms = b.tuned_ms(index);
+    out->col_tma = e.col_tma() && e.col_tma_applies() ? 1 : 0;
+    out->crt_tm = e.crt_tm() ? 1 : 0;
+    out->launch_groups = b.launch_groups(index);
     return PM_OK;
 }
 

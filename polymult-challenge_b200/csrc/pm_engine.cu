@@ -198,8 +198,9 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
         }
         if (crt_tc_) smem_crt_ = crt_tc_smem(dp_);
         // the single-tile CRT with its A operand in tensor memory where it applies (POLYMULT_CRT_TM)
-        crt_tm_ = POLYMULT_CRT_TM && crt_tc_ && plan_.KP <= 128 && dp_.crt_nrows <= 256 &&
-                  dp_.crt_kbytes <= 512 && crt_tm_smem(dp_) <= smem_optin_;
+        crt_tm_ok_ = crt_tc_ && plan_.KP <= 128 && dp_.crt_nrows <= 256 && dp_.crt_kbytes <= 512 &&
+                     crt_tm_smem(dp_) <= smem_optin_;
+        crt_tm_ = POLYMULT_CRT_TM && crt_tm_ok_;
         // multiplies per launch group of run_device: up to POLYMULT_GROUP_WORDS residue words
         // per operand (default 64 Mi: 8 multiplies at N = 65536, W = 1747, 512 MB of residue
         // scratch), at most 256.  Measured there: 1 multiply per group 4083 mults/s, 2 4789,
@@ -742,6 +743,16 @@ void Engine::reserve_crt_partials(size_t coeffs) {
     cuda_check(cudaMalloc(&d_zp_, coeffs * crt_zl(plan_.L) * 4), "cudaMalloc CRT partials");
     cuda_check(cudaMalloc(&d_sp_, coeffs * 4), "cudaMalloc CRT partials");
     partial_coeffs_ = coeffs;
+}
+
+void Engine::set_variant(bool col_tma, bool crt_tm) {
+    dp_.col_tma = col_tma ? 1 : 0;
+    crt_tm_ = crt_tm && crt_tm_ok_;
+}
+
+bool Engine::col_tma_applies() const {
+    // the TMA column pass: lines of 256 rows, tiles of 64 columns (launch_cols_tma)
+    return plan_.w1 == 8 && plan_.ncols >= 64;
 }
 
 int Engine::kernel_launches_per_group() const {

@@ -98,6 +98,16 @@ class Engine {
     // failed device-side check would.
     void set_status_for_test(uint32_t bits);
 
+    // Kernel variants the batch autotuner chooses between: the column passes of 256-row lines by
+    // the TMA-pipelined kernel or one tile per CTA; the single-tile CRT GEMM with its A operand
+    // in tensor memory (k_crt_tm) or in shared memory (k_crt_tc).  A variant that does not
+    // apply to the point is ignored.
+    void set_variant(bool col_tma, bool crt_tm);
+    bool col_tma() const { return dp_.col_tma != 0; }
+    bool crt_tm() const { return crt_tm_; }
+    bool col_tma_applies() const;
+    bool crt_tm_applies() const { return crt_tm_ok_; }
+
     const Plan& plan() const { return plan_; }
     const DevPlan& dev() const { return dp_; }
     int gemm_form() const { return form_; }
@@ -170,6 +180,7 @@ class Engine {
     int form_ = GEMM_PLAIN;
     bool dec_tc_ = false, crt_tc_ = false;  // which contractions run on the tensor cores
     bool crt_tm_ = false;                   // the single-tile CRT takes k_crt_tm (A in tensor memory)
+    bool crt_tm_ok_ = false;                // k_crt_tm applies to this point
     bool crt_blocked_ = false;              // the tensor-core CRT runs in blocks (K > one tile)
     std::vector<DecBlock> dec_blocks_;
     std::vector<CrtBlock> crt_blocks_;

@@ -68,7 +68,8 @@ class PmBatchInfo(ctypes.Structure):
 
 class PmBatchClassInfo(ctypes.Structure):
     _fields_ = [("K", ctypes.c_int32), ("w1", ctypes.c_int32), ("w2", ctypes.c_int32),
-                ("gemm_form", ctypes.c_int32), ("tuned_ms", ctypes.c_double)]
+                ("gemm_form", ctypes.c_int32), ("tuned_ms", ctypes.c_double),
+                ("col_tma", ctypes.c_int32), ("crt_tm", ctypes.c_int32), ("launch_groups", ctypes.c_uint32)]
 
 
 BATCH_TUNE, BATCH_NO_GRAPH = 1, 2

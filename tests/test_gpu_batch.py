@@ -4,7 +4,8 @@ CUDA-graph launch, with explicit and autotuned 4-step splits and GEMM forms.
 Every output is compared bit-for-bit with the single-point device path (pm_run_device, whose
 parity against the reference's own outputs is tests/test_gpu_parity.py) and, for the small
 classes, with the C oracle.  Also: graph replays rewrite their outputs, every valid split of a
-point gives the same bytes, the tuner's cache is written and read back, and line lengths up to
+point and every kernel variant and launch-group count the tuner chooses from gives the same
+bytes, the tuner's cache is written and read back, and line lengths up to
 2^10 (N = 2^18 .. 2^20, the three-phase and two-warp-row NTT forms) against the C oracle."""
 import os
 
@@ -133,14 +134,19 @@ def test_autotuner_chooses_and_caches(tmp_path, monkeypatch):
     ensure_library()
     cache = tmp_path / "tune.txt"
     monkeypatch.setenv("POLYMULT_TUNE_CACHE", str(cache))
-    ks = [_class(torch, N, W, c, seed=50 + i) for i, (N, W, c) in enumerate([(4096, 256, 3), (16384, 868, 2)])]
+    ks = [_class(torch, N, W, c, seed=50 + i)
+          for i, (N, W, c) in enumerate([(4096, 256, 3), (16384, 868, 2), (65536, 1747, 2)])]
     want = [_single(torch, k) for k in ks]
     with polymult.Batch([_spec(k) for k in ks], tune=True) as b:
+        chosen = []
         for i, k in enumerate(ks):
             ci = b.class_info(i)
             logN = k["N"].bit_length() - 1
             assert logN // 2 - 1 <= ci["w1"] <= logN // 2 + 1
             assert ci["tuned_ms"] > 0
+            assert ci["launch_groups"] in (1, 2, 4) and ci["launch_groups"] <= k["count"]
+            assert ci["col_tma"] in (0, 1) and ci["crt_tm"] in (0, 1)
+            chosen.append((ci["w1"], ci["gemm_form"], ci["col_tma"], ci["crt_tm"], ci["launch_groups"]))
         for k in ks:
             k["c"].zero_()
         b.run(torch.cuda.current_stream().cuda_stream)
@@ -148,9 +154,39 @@ def test_autotuner_chooses_and_caches(tmp_path, monkeypatch):
         for k, w in zip(ks, want):
             assert np.array_equal(k["c"].cpu().numpy().view(np.uint32), w)
     lines = cache.read_text().strip().splitlines()
-    assert len(lines) == 2
+    assert len(lines) == 3 and all(len(ln.split()) == 10 for ln in lines)
     with polymult.Batch([_spec(k) for k in ks], tune=True) as b2:  # served from the cache
-        assert all(b2.class_info(i)["tuned_ms"] == -1.0 for i in range(len(ks)))
+        for i in range(len(ks)):
+            ci = b2.class_info(i)
+            assert ci["tuned_ms"] == -1.0
+            assert (ci["w1"], ci["gemm_form"], ci["col_tma"], ci["crt_tm"], ci["launch_groups"]) == chosen[i]
+
+
+@pytest.mark.parametrize("col_tma,crt_tm,groups", [(1, 1, 1), (0, 1, 2), (1, 0, 4), (0, 0, 1)])
+def test_every_kernel_variant_gives_the_same_bytes(tmp_path, monkeypatch, col_tma, crt_tm, groups):
+    """Each variant the tuner can choose -- the column pass by the TMA pipeline or one tile per
+    CTA, the CRT's A operand in tensor or shared memory, the class in 1, 2 or 4 launch groups --
+    forced through a cache entry, gives the single-point path's bytes.  An entry in the older
+    seven-field form is read with the engine's default variants and one launch group."""
+    torch = _torch()
+    import polymult
+    ensure_library()
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("POLYMULT_TUNE_CACHE", str(cache))
+    dev = torch.cuda.get_device_name(0).replace(" ", "_")
+    ks = [_class(torch, 65536, 1747, 4, seed=70), _class(torch, 4096, 868, 4, seed=71)]
+    want = [_single(torch, k) for k in ks]
+    cache.write_text("65536 1747 4 %s 0 8 1.0 %d %d %d\n4096 868 4 %s 0 6 1.0\n"
+                     % (dev, col_tma, crt_tm, groups, dev))
+    with polymult.Batch([_spec(k) for k in ks], tune=True) as b:
+        ci = b.class_info(0)
+        assert (ci["w1"], ci["col_tma"], ci["crt_tm"], ci["launch_groups"]) == (8, col_tma, crt_tm, groups)
+        assert b.class_info(1)["launch_groups"] == 1
+        assert b.info()["kernel_launches"] >= groups * 8
+        b.run(torch.cuda.current_stream().cuda_stream)
+        b.sync()
+        for k, w in zip(ks, want):
+            assert np.array_equal(k["c"].cpu().numpy().view(np.uint32), w)
 
 
 @pytest.mark.parametrize("N,W", [(1 << 17, 64), (1 << 18, 100), (1 << 20, 64)])
