@@ -620,13 +620,16 @@ __global__ void __launch_bounds__(256, 3) k_ntt_cols2(DevPlan P, uint32_t* __res
 template <int NB>
 struct ColtCfg {
     static constexpr int NR = 1 << NB;
+    static constexpr int TC = 64;                     // tile columns (64 or 32)
+    static constexpr int LPR = TC / 2;                // lanes per tile row (two columns each)
+    static constexpr int GPW = 32 / LPR;              // element groups a warp covers at once
     static constexpr int GROUPS = 2;                  // consumer groups, each on its own tiles
     static constexpr int GROUP_WARPS = 8;
     static constexpr int GROUP_THREADS = 32 * GROUP_WARPS;
     static constexpr int THREADS = GROUPS * GROUP_THREADS + 32;
-    static constexpr int TILE_BYTES = NR * COL2_TC * 4;
+    static constexpr int TILE_BYTES = NR * TC * 4;
     static constexpr int SLOT_BYTES = TILE_BYTES + NR * 8;  // tile, then the prime's twiddles
-    static constexpr int STAGES = 3;                  // slots: 198 KB
+    static constexpr int STAGES = TC == 64 ? 3 : 6;   // slots: 198 / 204 KB
     static constexpr size_t SMEM = 128 + (size_t)STAGES * SLOT_BYTES;  // barriers, then the slots
     static constexpr int MIN_BLOCKS = 1;
     static_assert(SLOT_BYTES % 128 == 0, "slots stay 128-byte aligned");
@@ -639,15 +642,17 @@ __device__ __forceinline__ void colt_phase(uint32_t* tile, const Tw2* tws, uint3
     constexpr int b0 = C::b0(K);
     constexpr int NGRP = (1 << NB) / C::E;  // element groups per column
     constexpr bool LAST = INV ? K == 0 : K == C::NPH - 1;
-    const int c2 = 2 * (int)(threadIdx.x & 31);
-    static_assert(NGRP % ColtCfg<NB>::GROUP_WARPS == 0, "every warp takes whole element groups");
+    using G = ColtCfg<NB>;
+    const int lane = (int)(threadIdx.x & 31);
+    const int c2 = 2 * (lane % G::LPR);
+    static_assert(NGRP % (G::GROUP_WARPS * G::GPW) == 0, "every warp takes whole element groups");
 #pragma unroll 1
-    for (int gidx = gw; gidx < NGRP; gidx += ColtCfg<NB>::GROUP_WARPS) {
+    for (int gidx = gw * G::GPW + lane / G::LPR; gidx < NGRP; gidx += G::GROUP_WARPS * G::GPW) {
         const int lo = gidx & ((1 << b0) - 1), hip = gidx >> b0;
         const int xb = (hip << (b0 + C::RB)) | lo;
         // element e of the group is row xb + (e << b0)
-        uint2* sb = reinterpret_cast<uint2*>(tile + xb * COL2_TC + c2);
-        constexpr int sstep = (COL2_TC << b0) / 2;
+        uint2* sb = reinterpret_cast<uint2*>(tile + xb * G::TC + c2);
+        constexpr int sstep = (G::TC << b0) / 2;
         uint32_t v[C::E], u[C::E];
 #pragma unroll
         for (int e = 0; e < C::E; ++e) {
@@ -723,7 +728,7 @@ __global__ void __launch_bounds__(ColtCfg<NB>::THREADS, ColtCfg<NB>::MIN_BLOCKS)
                 const uint32_t unit = t / tiles_x, tx = t - unit * tiles_x, j = unit % P.K;
                 unsigned char* slot = smem_raw + 128 + (size_t)s * G::SLOT_BYTES;
                 mbar_arrive_expect_tx(full + s, G::SLOT_BYTES);
-                tma_load_2d(slot, &tmap, (int)(col0 + tx * COL2_TC), (int)(unit << NB), full + s);
+                tma_load_2d(slot, &tmap, (int)(col0 + tx * G::TC), (int)(unit << NB), full + s);
                 bulk_g2s(slot + G::TILE_BYTES, P.tw + (size_t)j * P.N, G::NR * 8, full + s);
             }
             // every copy issued into a slot lands before the CTA exits (the latest per slot)
@@ -742,7 +747,7 @@ __global__ void __launch_bounds__(ColtCfg<NB>::THREADS, ColtCfg<NB>::MIN_BLOCKS)
             const uint32_t unit = t / tiles_x, tx = t - unit * tiles_x, j = unit % P.K;
             unsigned char* slot = smem_raw + 128 + (size_t)s * G::SLOT_BYTES;
             colt_phases<NB, INV, 0>(reinterpret_cast<uint32_t*>(slot), reinterpret_cast<const Tw2*>(slot + G::TILE_BYTES),
-                                    R + (size_t)unit * P.N + col0 + tx * COL2_TC, P.ncols, P.p[j], grp, gw);
+                                    R + (size_t)unit * P.N + col0 + tx * G::TC, P.ncols, P.p[j], grp, gw);
             fence_smem_to_async();  // the in-place phase-0 writes, before the slot's next TMA load
             __syncwarp();
             if ((threadIdx.x & 31) == 0) mbar_arrive(empty + s);
@@ -815,19 +820,20 @@ bool launch_cols_tma(bool inv, dim3 grid, cudaStream_t s, const DevPlan& P, uint
     // lines of 256 rows only: at 128 rows (N = 32768) the one-tile-per-CTA kernel, three CTAs per
     // SM, measured faster (3.33 against 3.39 us per pass at W = 868)
     if constexpr (NB == 8) {
-        if (!P.col_tma || ltc < 6 || col0 % COL2_TC != 0 || P.nrows != (1u << NB)) return false;
+        using G = ColtCfg<NB>;
+        const uint32_t cw = grid.x << ltc;
+        if (!P.col_tma || cw % G::TC != 0 || col0 % G::TC != 0 || P.nrows != (1u << NB)) return false;
         const auto enc = tensor_map_encoder();
         if (!enc) return false;
-        using G = ColtCfg<NB>;
-        const uint32_t tiles_x = grid.x << (ltc - 6);
+        const uint32_t tiles_x = cw / G::TC;
         const uint64_t lines = (uint64_t)grid.y * grid.z;
         const uint64_t ntiles = tiles_x * lines;
         if (ntiles == 0) return true;
-        // R as a [lines * nrows][ncols] matrix of u32, boxes of [2^NB rows][64 columns]
+        // R as a [lines * nrows][ncols] matrix of u32, boxes of [2^NB rows][TC columns]
         CUtensorMap m;
         const cuuint64_t dims[2] = {P.ncols, lines * P.nrows};
         const cuuint64_t strides[1] = {(cuuint64_t)P.ncols * 4};
-        const cuuint32_t box[2] = {(cuuint32_t)COL2_TC, (cuuint32_t)G::NR};
+        const cuuint32_t box[2] = {(cuuint32_t)G::TC, (cuuint32_t)G::NR};
         const cuuint32_t es[2] = {1, 1};
         if (ntiles > 0xFFFFFFFFull || lines * P.nrows > 0x7FFFFFFFull ||
             enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, R, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
