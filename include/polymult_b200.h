@@ -225,13 +225,19 @@ typedef struct pm_pipeline_info {
 /* No reference counterpart: the autotuner of the host pipeline.  Runs `reps` pm_run calls (plus
  * a warm-up) for every schedule with body divisors in {1, 2, 4, 8, 16} x {1, 2, 4, 8, 16} on
  * pageable timing buffers (narrow head chunks only with a body of 8 or more; with
- * PM_PIPELINE_PINNED: {1, 2, 3, 4, 8, 16} squared on page-locked ones, 3 standing for the chunks
- * 1/2, 1/4, 1/4 of b and 1/4, 1/4, 1/2 of c), keeps the one with the lowest median wall time for
- * that kind of call, and describes it in *out.  Before any tuning the schedules follow the
- * operand size (one chunk below 1 MB, quarters below 8 MB, eighths above).  Synchronous; up to
- * 25 (PM_PIPELINE_PINNED: 36) x (reps + 1) calls. */
+ * PM_PIPELINE_PINNED: {1, 2, 3, 4, 5, 8, 16} squared on page-locked ones, 3 standing for the
+ * chunks 1/2, 1/4, 1/4 of b and 1/4, 1/4, 1/2 of c, and 5 for 1/2, 1/4, 1/8, 1/8 of b and
+ * 1/8, 1/8, 1/4, 1/2 of c), keeps the one with the lowest median wall time for that kind of
+ * call, and describes it in *out.  Before any tuning the schedules follow the operand size (one
+ * chunk below 1 MB, quarters below 8 MB, eighths above).  Synchronous; up to 25
+ * (PM_PIPELINE_PINNED: 49) x (reps + 1) calls. */
 int pm_tune_pipeline(pm_context* ctx, int reps, int flags, pm_pipeline_info* out);
 int pm_get_pipeline(const pm_context* ctx, int flags, pm_pipeline_info* out);
+/* No reference counterpart: sets the schedule of one kind of call (flags as above) to body
+ * divisors `in_body` / `out_body` -- powers of two up to ncols, or for PM_PIPELINE_PINNED also
+ * 3 and 5 (the uneven shapes of pm_tune_pipeline) -- without measuring, e.g. to reuse a
+ * schedule tuned earlier.  PM_ERR_INVALID for another divisor. */
+int pm_set_pipeline(pm_context* ctx, int flags, int32_t in_body, int32_t out_body);
 
 /* Waits for the context's device work and returns PM_ERR_DEVICE if a device-side check
  * failed since the last call. */

@@ -189,6 +189,19 @@ int pm_tune_pipeline(pm_context* ctx, int reps, int flags, pm_pipeline_info* out
     });
 }
 
+int pm_set_pipeline(pm_context* ctx, int flags, int32_t in_body, int32_t out_body) {
+    if (!ctx || !ctx->engine) return fail(PM_ERR_INVALID, "null context");
+    if (flags & ~PM_PIPELINE_PINNED) return fail(PM_ERR_INVALID, "unknown pipeline flags");
+    if (in_body <= 0 || out_body <= 0) return fail(PM_ERR_INVALID, "chunk divisors must be positive");
+    const int kind = (flags & PM_PIPELINE_PINNED) ? 1 : 0;
+    const uint32_t nc = ctx->engine->plan().ncols;
+    if ((uint32_t)in_body > nc || (uint32_t)out_body > nc) return fail(PM_ERR_INVALID, "chunk divisor above ncols");
+    return guarded([&] {
+        ctx->engine->set_chunk_schedule((uint32_t)in_body, (uint32_t)out_body, kind);
+        ctx->tuned_ms[kind] = 0.0;
+    });
+}
+
 int pm_get_pipeline(const pm_context* ctx, int flags, pm_pipeline_info* out) {
     if (!ctx || !ctx->engine || !out) return fail(PM_ERR_INVALID, "null argument");
     if (flags & ~PM_PIPELINE_PINNED) return fail(PM_ERR_INVALID, "unknown pipeline flags");

@@ -407,12 +407,14 @@ void Engine::ensure_scratch(uint32_t group) {
 // sized for the longer schedule.
 // Direct-copy calls also take divisor 3 for either side: b in [1/2, 1/4, 1/4] (the last chunk,
 // whose compute is exposed, a quarter) and the output in [1/4, 1/4, 1/2] (the first, which gates
-// the first D2H, a quarter) -- three copies each.
+// the first D2H, a quarter) -- three copies each; and divisor 5, geometric: b in
+// [1/2, 1/4, 1/8, 1/8] and the output in [1/8, 1/8, 1/4, 1/2] -- four copies each, an eighth of
+// the transform exposed at either end of the device tail.
 void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind) {
     if (kind != 0 && kind != 1) throw InvalidPoint("pipeline kind must be 0 (staged) or 1 (direct)");
-    auto ok = [&](uint32_t d) { return d != 0 && ((d & (d - 1)) == 0 || (kind == 1 && d == 3)); };
+    auto ok = [&](uint32_t d) { return d != 0 && ((d & (d - 1)) == 0 || (kind == 1 && (d == 3 || d == 5))); };
     if (!ok(in_body) || !ok(out_body))
-        throw InvalidPoint("chunk divisors must be powers of two (or 3 for direct-copy calls)");
+        throw InvalidPoint("chunk divisors must be powers of two (or 3 or 5 for direct-copy calls)");
     const uint32_t nc = plan_.ncols;
     if (kind == 0) {
         // narrow head (and output tail) chunks only under a fine body: they start the staging
@@ -420,8 +422,12 @@ void Engine::set_chunk_schedule(uint32_t in_body, uint32_t out_body, int kind) {
         cin_[kind] = in_body >= 8 ? make_chunks(nc, {32, 32, 16}, in_body, {}) : make_chunks(nc, {}, in_body, {});
         cout_[kind] = out_body >= 8 ? make_chunks(nc, {64, 32}, out_body, {32, 64}) : make_chunks(nc, {}, out_body, {});
     } else {
-        cin_[kind] = in_body == 3 ? make_chunks(nc, {2}, 4, {}) : make_chunks(nc, {}, in_body, {});
-        cout_[kind] = out_body == 3 ? make_chunks(nc, {}, 4, {2}) : make_chunks(nc, {}, out_body, {});
+        cin_[kind] = in_body == 3   ? make_chunks(nc, {2}, 4, {})
+                     : in_body == 5 ? make_chunks(nc, {2, 4, 8}, 8, {})
+                                    : make_chunks(nc, {}, in_body, {});
+        cout_[kind] = out_body == 3   ? make_chunks(nc, {}, 4, {2})
+                      : out_body == 5 ? make_chunks(nc, {8}, 8, {4, 2})
+                                      : make_chunks(nc, {}, out_body, {});
     }
     in_body_[kind] = in_body;
     out_body_[kind] = out_body;
@@ -466,15 +472,15 @@ double Engine::tune_host_pipeline(int reps, int kind) {
     for (size_t i = 0; i < words; ++i) a[i] = (i % plan_.L == plan_.L - 1) ? 0u : (uint32_t)(i * 2654435761u);
     double best = 1e30;
     uint32_t bi = in_body_[kind], bo = out_body_[kind];
-    // body divisors: 4, 8, 16; direct-copy calls also 2 and 3 (fewer copies, each ~4 us of DMA
-    // set-up, against more compute exposed after the last input chunk and before the first output
-    // one; 3: the uneven three-chunk shapes of set_chunk_schedule)
-    const uint32_t cand[6] = {1, 2, 3, 4, 8, 16};
+    // body divisors 1, 2, 4, 8, 16; direct-copy calls also 3 and 5 (the uneven three- and
+    // four-chunk shapes of set_chunk_schedule): fewer copies, each ~4 us of DMA set-up, against
+    // more compute exposed after the last input chunk and before the first output one
+    const uint32_t cand[7] = {1, 2, 3, 4, 5, 8, 16};
     try {
         for (uint32_t ib : cand)
             for (uint32_t ob : cand) {
-                if (ib > plan_.ncols || ob > plan_.ncols) continue;
-                if (kind == 0 && (ib == 3 || ob == 3)) continue;
+                if ((ib == 5 ? 8 : ib) > plan_.ncols || (ob == 5 ? 8 : ob) > plan_.ncols) continue;
+                if (kind == 0 && (ib == 3 || ob == 3 || ib == 5 || ob == 5)) continue;
                 set_chunk_schedule(ib, ob, kind);
                 run_host(a, a, c);
                 std::vector<double> t;

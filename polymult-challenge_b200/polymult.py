@@ -128,6 +128,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_selftest_host_pool.restype = ctypes.c_int
     lib.pm_tune_pipeline.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
     lib.pm_tune_pipeline.restype = ctypes.c_int
+    lib.pm_set_pipeline.argtypes = [vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32]
+    lib.pm_set_pipeline.restype = ctypes.c_int
     lib.pm_get_pipeline.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PmPipelineInfo)]
     lib.pm_get_pipeline.restype = ctypes.c_int
     lib.pm_batch_init.argtypes = [ctypes.POINTER(PmBatchClass), ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
@@ -273,6 +275,10 @@ class Multiplier:
         inf = PmPipelineInfo()
         _check(load().pm_tune_pipeline(self._h, reps, PIPELINE_PINNED if pinned else 0, ctypes.byref(inf)))
         return {f: getattr(inf, f) for f, _ in PmPipelineInfo._fields_}
+
+    def set_pipeline(self, in_body: int, out_body: int, pinned: bool = False):
+        """Sets the chunk schedule of one kind of call without measuring (pm_set_pipeline)."""
+        _check(load().pm_set_pipeline(self._h, PIPELINE_PINNED if pinned else 0, in_body, out_body))
 
     def pipeline(self, pinned: bool = False) -> dict:
         inf = PmPipelineInfo()

@@ -117,4 +117,5 @@ def test_batch_server_pipeline_argument_checks():
     assert lib.pm_tune_pipeline(None, 3, 0, None) == polymult.PM_ERR_INVALID
     assert lib.pm_tune_pipeline(None, 3, polymult.PIPELINE_PINNED, None) == polymult.PM_ERR_INVALID
     assert lib.pm_get_pipeline(None, 0, None) == polymult.PM_ERR_INVALID
+    assert lib.pm_set_pipeline(None, 0, 8, 8) == polymult.PM_ERR_INVALID
 

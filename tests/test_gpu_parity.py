@@ -181,12 +181,40 @@ def test_tuned_pipeline_still_bit_exact():
         # the page-locked schedule is tuned on its own and leaves the staged one alone
         assert m.pipeline(pinned=True)["tuned_ms"] == 0
         pinfo = m.tune_pipeline(2, pinned=True)
-        assert pinfo["in_body"] in (1, 2, 3, 4, 8, 16) and pinfo["out_body"] in (1, 2, 3, 4, 8, 16)
+        assert pinfo["in_body"] in (1, 2, 3, 4, 5, 8, 16) and pinfo["out_body"] in (1, 2, 3, 4, 5, 8, 16)
         assert pinfo["tuned_ms"] > 0
         assert m.pipeline(pinned=True) == pinfo and m.pipeline() == info
         for case in pt["cases"]:
             a, b, _ = regen_case(pt, case)
             assert sha(m.multiply(a, b)) == case["c_sha256"], (case["s"], case["mode"])
+        m.sync()
+
+
+@pytest.mark.parametrize("shape", [(3, 3), (5, 5), (5, 1), (1, 5), (16, 2)], ids=lambda x: "in%d_out%d" % x)
+def test_every_pinned_chunk_shape_is_bit_exact(shape):
+    """Each schedule pm_tune_pipeline can choose for page-locked calls, set directly with
+    pm_set_pipeline -- the uneven shapes 3 (b in halves and quarters) and 5 (b in 1/2, 1/4,
+    1/8, 1/8; c in 1/8, 1/8, 1/4, 1/2) included -- gives the reference's bytes; divisors outside
+    the candidates are refused."""
+    torch = _torch()
+    import polymult
+    pt = next(p for p in POINTS if (p["N"], p["W"]) == (65536, 1747))
+    with _multiplier(pt, "tensor") as m:
+        m.set_pipeline(shape[0], shape[1], pinned=True)
+        info = m.pipeline(pinned=True)
+        assert (info["in_body"], info["out_body"]) == shape and info["tuned_ms"] == 0
+        with pytest.raises(polymult.PolymultError):
+            m.set_pipeline(5, 5)  # the uneven shapes are for page-locked calls only
+        with pytest.raises(polymult.PolymultError):
+            m.set_pipeline(6, 8, pinned=True)
+        L = (pt["W"] + 31) // 32
+        for case in pt["cases"][:2]:
+            a, b, _ = regen_case(pt, case)
+            pa, pb, pc = (torch.empty((pt["N"], L), dtype=torch.int32).pin_memory() for _ in range(3))
+            pa.numpy().view(np.uint32)[:] = a
+            pb.numpy().view(np.uint32)[:] = b
+            m.multiply(pa.numpy().view(np.uint32), pb.numpy().view(np.uint32), pc.numpy().view(np.uint32))
+            assert sha(pc.numpy().view(np.uint32)) == case["c_sha256"], (shape, case["s"])
         m.sync()
 
 
