@@ -799,18 +799,24 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     achieved = alg / (stages[dom] / 1000.0) / 1e9
     traffic = None
+    pipes = None
     tfile = os.path.join(REPO, "profiles", "traffic_bytes.json")
     if os.path.exists(tfile):
         try:
-            tt = json.load(open(tfile)).get(info["gemm"], {})
+            tj = json.load(open(tfile))
+            tt = tj.get(info["gemm"], {})
             t1 = tt.get(dom)
             # captured on launches of tt["multiplies_per_launch"] multiplies; scaled to B
             traffic = None if t1 is None else int(t1 * B / tt.get("multiplies_per_launch", 1))
+            pipes = tj.get("pipes", {}).get(info["gemm"], {}).get(dom)
         except Exception:
             traffic = None
     roofline = {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes": alg, "kernel_ms": round(stages[dom], 4), "multiplies_per_launch": B}
+    if pipes:
+        # the unit that binds the kernel, from the committed ncu capture (HBM is not it here)
+        roofline["binding_pipe"] = pipes
     whole = {"algorithmic_bytes_per_multiply": (12 * N * L + 24 * K * N), "ms_per_multiply": round(ms / args.steps / B, 5)}
     whole["achieved_gbs"] = round(whole["algorithmic_bytes_per_multiply"] / (whole["ms_per_multiply"] / 1000.0) / 1e9, 1)
     whole["frac_of_hbm"] = round(whole["achieved_gbs"] / peak, 4)
