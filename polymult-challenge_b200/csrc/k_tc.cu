@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                         const int jb = j0 + 4 * (c16 + DEC_SUBS * u);
                         uint32_t* out = Rb + (size_t)jb * P.N;
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
+                        for (int q = 0; q < 4; ++q, out += P.N) {
                             const uint32_t p = pc[u][q].x, pinv = pc[u][q].y;
                             const uint32_t* rq = &r[u][4 * q];
                             uint32_t y;
@@ -384,13 +384,13 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                                 // x = t0 + t1 2^16 (one wide multiply-add) with t0 = r0 + r1 2^8 and t1 = r2 + r3 2^8
                                 // below 2^32
                                 const uint32_t t0 = rq[0] + (rq[1] << 8), t1 = rq[2] + (rq[3] << 8);
-                                y = redc64((uint64_t)t1 * 65536u + t0, p, pinv);
+                                y = redc64(((uint64_t)t1 << 16) + t0, p, pinv);
                             } else {
                                 const uint64_t x = (uint64_t)rq[0] + ((uint64_t)rq[1] << 8) + ((uint64_t)rq[2] << 16) +
                                                    ((uint64_t)rq[3] << 24);
                                 y = redc64(x, p, pinv);
                             }
-                            if (st && jb + q < P.K) out[(size_t)q * P.N] = y;
+                            if (st && jb + q < P.K) *out = y;
                         }
                     }
                 }

@@ -89,10 +89,11 @@ __device__ __forceinline__ uint32_t mont_mul(uint32_t a, uint32_t b, uint32_t p,
     return (uint32_t)(t >> 32) - __umulhi(m, p) + p;
 }
 
-// t * 2^-32 mod p in (0, 2p) for a 64-bit t < p * 2^32.
+// t * 2^-32 mod p in (0, 2p) for a 64-bit t < p * 2^32 (the high product from one 64-bit
+// multiply, as in mont_mul).
 __device__ __forceinline__ uint32_t redc64(uint64_t t, uint32_t p, uint32_t pinv) {
     const uint32_t m = (uint32_t)t * pinv;
-    return (uint32_t)(t >> 32) - __umulhi(m, p) + p;
+    return (uint32_t)(t >> 32) - (uint32_t)(((uint64_t)m * p) >> 32) + p;
 }
 
 // [0, 2m) -> [0, m) (also [0, 4p) -> [0, 2p) with m = 2p): unsigned min of x and x - m (one
