@@ -635,9 +635,10 @@ struct ColtCfg {
     static_assert(SLOT_BYTES % 128 == 0, "slots stay 128-byte aligned");
 };
 
-template <int NB, bool INV, int K>
-__device__ __forceinline__ void colt_phase(uint32_t* tile, const Tw2* tws, uint32_t* gout, uint32_t ncols, uint32_t p,
+template <int NB, bool INV, int K, int GL>
+__device__ __forceinline__ void colt_phase(uint32_t* tile, const Tw2* tws, uint32_t* gout, uint32_t ncols_rt, uint32_t p,
                                            int gw) {
+    const uint32_t ncols = GL >= 0 ? (1u << (GL >= 0 ? GL : 0)) : ncols_rt;
     using C = LineCfg<NB>;
     constexpr int b0 = C::b0(K);
     constexpr int NGRP = (1 << NB) / C::E;  // element groups per column
@@ -683,22 +684,24 @@ __device__ __forceinline__ void colt_phase(uint32_t* tile, const Tw2* tws, uint3
     }
 }
 
-template <int NB, bool INV, int I>
+template <int NB, bool INV, int I, int GL>
 __device__ __forceinline__ void colt_phases(uint32_t* tile, const Tw2* tws, uint32_t* gout, uint32_t ncols, uint32_t p,
                                             int grp, int gw) {
     using C = LineCfg<NB>;
     if constexpr (I < C::NPH) {
         constexpr int K = INV ? C::NPH - 1 - I : I;
-        colt_phase<NB, INV, K>(tile, tws, gout, ncols, p, gw);
+        colt_phase<NB, INV, K, GL>(tile, tws, gout, ncols, p, gw);
         if constexpr (I + 1 < C::NPH) {
             named_sync(1 + grp, ColtCfg<NB>::GROUP_THREADS);
-            colt_phases<NB, INV, I + 1>(tile, tws, gout, ncols, p, grp, gw);
+            colt_phases<NB, INV, I + 1, GL>(tile, tws, gout, ncols, p, grp, gw);
         }
     }
 }
 
-// tile t: columns col0 + 64 (t mod tiles_x) .., line (batch entry, prime) unit = t / tiles_x
-template <int NB, bool INV>
+// tile t: columns col0 + TC (t mod tiles_x) .., line (batch entry, prime) unit = t / tiles_x.
+// GL >= 0: log2 of the row pitch ncols at compile time (the last phase's stores then address
+// their rows with immediates); -1: the pitch at run time.
+template <int NB, bool INV, int GL>
 __global__ void __launch_bounds__(ColtCfg<NB>::THREADS, ColtCfg<NB>::MIN_BLOCKS)
     k_ntt_cols_tma(const __grid_constant__ CUtensorMap tmap, DevPlan P, uint32_t* __restrict__ R, uint32_t col0,
                    uint32_t tiles_x, uint32_t ntiles) {
@@ -746,7 +749,7 @@ __global__ void __launch_bounds__(ColtCfg<NB>::THREADS, ColtCfg<NB>::MIN_BLOCKS)
             if (named_sync_or(1 + G::GROUPS + grp, G::GROUP_THREADS, !ok)) break;  // the group leaves together
             const uint32_t unit = t / tiles_x, tx = t - unit * tiles_x, j = unit % P.K;
             unsigned char* slot = smem_raw + 128 + (size_t)s * G::SLOT_BYTES;
-            colt_phases<NB, INV, 0>(reinterpret_cast<uint32_t*>(slot), reinterpret_cast<const Tw2*>(slot + G::TILE_BYTES),
+            colt_phases<NB, INV, 0, GL>(reinterpret_cast<uint32_t*>(slot), reinterpret_cast<const Tw2*>(slot + G::TILE_BYTES),
                                     R + (size_t)unit * P.N + col0 + tx * G::TC, P.ncols, P.p[j], grp, gw);
             fence_smem_to_async();  // the in-place phase-0 writes, before the slot's next TMA load
             __syncwarp();
@@ -797,6 +800,17 @@ auto col2_kernel(int w2) {
     }
 }
 
+// the TMA column kernel for row pitch 2^w2 (compile-time pitch for w2 = 6 .. 9: N = 2^14 .. 2^17
+// at w1 = 8)
+template <bool INV>
+auto colt_kernel(int w2) {
+    if (w2 == 8) return k_ntt_cols_tma<8, INV, 8>;
+    if (w2 == 7) return k_ntt_cols_tma<8, INV, 7>;
+    if (w2 == 9) return k_ntt_cols_tma<8, INV, 9>;
+    if (w2 == 6) return k_ntt_cols_tma<8, INV, 6>;
+    return k_ntt_cols_tma<8, INV, -1>;
+}
+
 // cuTensorMapEncodeTiled from the driver (no link against libcuda); null if unavailable
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -845,7 +859,7 @@ bool launch_cols_tma(bool inv, dim3 grid, cudaStream_t s, const DevPlan& P, uint
                                                       cudaSuccess)
             throw_cuda(cudaGetLastError(), "device attributes");
         const uint32_t g = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)sms * G::MIN_BLOCKS);
-        const cudaError_t e = launch_kernel(inv ? k_ntt_cols_tma<NB, true> : k_ntt_cols_tma<NB, false>, dim3(g),
+        const cudaError_t e = launch_kernel(inv ? colt_kernel<true>(P.w2) : colt_kernel<false>(P.w2), dim3(g),
                                             dim3(G::THREADS), G::SMEM, s, pdl, m, P, R, col0, tiles_x, (uint32_t)ntiles);
         if (e != cudaSuccess) throw_cuda(e, inv ? "launch k_ntt_cols_tma<inverse>" : "launch k_ntt_cols_tma<forward>");
         return true;
@@ -945,7 +959,7 @@ struct ColAttrF {
             }
         }
         if constexpr (NB == 8) {
-            const void* ft[2] = {(const void*)k_ntt_cols_tma<NB, false>, (const void*)k_ntt_cols_tma<NB, true>};
+            const void* ft[2] = {(const void*)colt_kernel<false>(w2), (const void*)colt_kernel<true>(w2)};
             for (const void* f : ft) {
                 const cudaError_t e =
                     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ColtCfg<NB>::SMEM);
@@ -965,8 +979,8 @@ struct ColProbeF {
         }
         if constexpr (NB >= 7 && NB <= 8) {
             const void* f2[4] = {(const void*)col2_kernel<NB, false>(w2), (const void*)col2_kernel<NB, true>(w2),
-                                 NB == 8 ? (const void*)k_ntt_cols_tma<8, false> : nullptr,
-                                 NB == 8 ? (const void*)k_ntt_cols_tma<8, true> : nullptr};
+                                 NB == 8 ? (const void*)colt_kernel<false>(w2) : nullptr,
+                                 NB == 8 ? (const void*)colt_kernel<true>(w2) : nullptr};
             for (const void* f : f2) {
                 if (!f) continue;
                 cudaFuncAttributes fa{};
