@@ -54,7 +54,7 @@ RUNNER = os.path.join(PKG, "lib", "polymult_solution")
 sys.path.insert(0, PKG)
 
 N_RANK, W_RANK = 65536, 1747
-BATCH = 8
+BATCH = 32
 METRIC = "mults/s at N=65536 W=1747 (bit-exact): tensor-core+batched vs plain; p99 ms"
 L2_BYTES = 126 * 10**6
 
@@ -806,8 +806,11 @@ def run_ours(args):
             tj = json.load(open(tfile))
             tt = tj.get(info["gemm"], {})
             t1 = tt.get(dom)
-            # captured on launches of tt["multiplies_per_launch"] multiplies; scaled to B
-            traffic = None if t1 is None else int(t1 * B / tt.get("multiplies_per_launch", 1))
+            # captured on launches of a stated number of multiplies; scaled to B
+            if isinstance(t1, dict):
+                traffic = int(t1["bytes"] * B / t1.get("multiplies_per_launch", 1))
+            elif t1 is not None:
+                traffic = int(t1 * B / tt.get("multiplies_per_launch", 1))
             pipes = tj.get("pipes", {}).get(info["gemm"], {}).get(dom)
         except Exception:
             traffic = None

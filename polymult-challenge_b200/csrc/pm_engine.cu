@@ -202,11 +202,11 @@ Engine::Engine(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int gemm_r
                      crt_tm_smem(dp_) <= smem_optin_;
         crt_tm_ = POLYMULT_CRT_TM && crt_tm_ok_;
         // multiplies per launch group of run_device: up to POLYMULT_GROUP_WORDS residue words
-        // per operand (default 64 Mi: 8 multiplies at N = 65536, W = 1747, 512 MB of residue
-        // scratch), at most 256.  Measured there: 1 multiply per group 4083 mults/s, 2 4789,
-        // 8 5144 -- every kernel's fixed costs (B image, ramp, last partial wave) amortise over
-        // the group, which outweighs keeping one multiply's residues in L2.
-        size_t group_words = size_t(64) << 20;
+        // per operand (default 256 Mi: 32 multiplies at N = 65536, W = 1747, 2 GB of residue
+        // scratch), at most 256.  Measured there: 8 per group 9081 mults/s, 16 9435, 32 9646 --
+        // every kernel's fixed costs (B images, twiddle reads, ramp, last partial wave)
+        // amortise over the group.
+        size_t group_words = size_t(256) << 20;
         if (const char* e = std::getenv("POLYMULT_GROUP_WORDS")) group_words = std::max<size_t>(1, std::strtoull(e, nullptr, 10));
         const size_t per_mult = (size_t)plan_.K * plan_.N;
         group_cap_ = (uint32_t)std::max<size_t>(1, std::min<size_t>(256, group_words / std::max<size_t>(1, per_mult)));
