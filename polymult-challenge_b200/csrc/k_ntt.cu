@@ -362,10 +362,12 @@ __device__ __forceinline__ void row_inverse(uint32_t (&v)[RowCfg<NB>::E], uint32
 // compensates.  Blocks per SM: the most at which the variants do not spill (64 registers at 8,
 // 80 at 6, 128 at 4); the fused kernels hold the other operand's row and more twiddle runs.
 // The two-operand form at 6 (80 registers) ran its pass in 34.2 us per multiply against 36.1 at
-// 5 (96) and 37.4 at 4 (117) (N=65536, W=1747, launches of 8); at 7 it spills.
+// 5 (96) and 37.4 at 4 (117) (N=65536, W=1747, launches of 8); since the 64-bit product forms it
+// fits 7 (72 registers, no spill): 31.4 -> 31.0 us in launches of 32; at 8 (64) it spills.  The
+// fused form (host pipeline, server) keeps a 4-byte stack slot at 7 (8 bytes at 6).
 enum : int { ROWS_FWD = 0, ROWS_FUSED = 1, ROWS_BOTH = 2 };
 __host__ __device__ constexpr int rows_min_blocks(int nb, int mode) {
-    return nb >= 9 ? (mode == ROWS_FWD ? 5 : 4) : (mode == ROWS_FWD ? 8 : 6);
+    return nb >= 9 ? (mode == ROWS_FWD ? 5 : 4) : (mode == ROWS_FWD ? 8 : 7);
 }
 // POLYMULT_ROW_STATIC: the row kernels take the column-stage count w1 (and with it nrows and N)
 // as a template constant for the common splits, and a grid ordered (batch, row block, prime) so
