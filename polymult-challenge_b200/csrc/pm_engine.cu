@@ -525,6 +525,7 @@ void Engine::setup_host_pipeline() {
     *h_status_ = 0;
     profile_ = std::getenv("POLYMULT_PROFILE") != nullptr;
     if (const char* e = std::getenv("POLYMULT_GATHER_STORES")) nt_gather_ = std::strcmp(e, "cached") != 0;
+    if (const char* e = std::getenv("POLYMULT_MERGE_COPIES")) merge_copies_ = std::strcmp(e, "0") != 0;
     for (auto& s : s_comp_) cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_h2d_, cudaStreamNonBlocking), "stream");
     cuda_check(cudaStreamCreateWithFlags(&s_d2h_, cudaStreamNonBlocking), "stream");
@@ -1109,39 +1110,71 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     mark("start", s_h2d_);
     if (stage_start(0)) pool_->wait();
     t_stage0 = clk::now();
-    for (int i = 0; i < nin; ++i) {
-        const int P = items[i].first;
-        const Chunk ch = items[i].second;
-        const size_t off = (size_t)ch.col0 * nrows * L, words = (size_t)ch.cw * nrows * L;
-        // the next chunk is copied by the workers while this thread issues this one
-        const bool staging = i + 1 < nin && stage_start(i + 1);
+    // the kernels of input item k, once its copy is issued (the copy's event: ev_in_[hi])
+    auto issue_compute = [&](int k, int hi) {
+        const int P = items[k].first;
+        const Chunk ch = items[k].second;
+        const size_t off = (size_t)ch.col0 * nrows * L;
         // the last input chunk runs on stream 0, after a's row pass and b's other chunks, so
         // that its kernels, the fused row pass and the first output chunk's follow each other
         // in one stream (each launch overlapping the previous kernel's tail)
-        const bool last = i + 1 == nin;
-        cudaStream_t sc = last ? s_comp_[0] : s_comp_[i % 3];
+        const bool last = k + 1 == nin;
+        cudaStream_t sc = last ? s_comp_[0] : s_comp_[k % 3];
         if (last)
-            for (int k = na; k < i; ++k) cuda_check(cudaStreamWaitEvent(sc, ev_done_in_[k], 0), "wait");
-        if (direct_in[P])
-            cuda_check(cudaMemcpy2DAsync(d_in_[P] + off, (size_t)ch.cw * L * 4, src[P] + (size_t)ch.col0 * L, pitch,
-                                         (size_t)ch.cw * L * 4, nrows, cudaMemcpyHostToDevice, s_h2d_),
-                       "H2D");
-        else
-            cuda_check(cudaMemcpyAsync(d_in_[P] + off, h_in_[P] + off, words * 4, cudaMemcpyHostToDevice, s_h2d_),
-                       "H2D");
-        cuda_check(cudaEventRecord(ev_in_[i], s_h2d_), "record");
-        mark("h2d" + std::to_string(i), s_h2d_);
-        cuda_check(cudaStreamWaitEvent(sc, ev_in_[i], 0), "wait");
+            for (int q = na; q < k; ++q) cuda_check(cudaStreamWaitEvent(sc, ev_done_in_[q], 0), "wait");
+        cuda_check(cudaStreamWaitEvent(sc, ev_in_[hi], 0), "wait");
         launch_dec(d_in_[P] + off, ch, 1, dR[P], sc, P == 0);
         launch_cols(false, dR[P], ch, 1, sc, true);
         if (!last) {
-            cuda_check(cudaEventRecord(ev_done_in_[i], sc), "record");
-            mark("in" + std::to_string(i), sc);
+            cuda_check(cudaEventRecord(ev_done_in_[k], sc), "record");
+            mark("in" + std::to_string(k), sc);
         }
-        if (i == na - 1) {  // a complete: its row pass overlaps b's transfer
-            for (int k = 0; k < na; ++k) cuda_check(cudaStreamWaitEvent(s_comp_[0], ev_done_in_[k], 0), "wait");
+        if (k == na - 1) {  // a complete: its row pass overlaps b's transfer
+            for (int q = 0; q < na; ++q) cuda_check(cudaStreamWaitEvent(s_comp_[0], ev_done_in_[q], 0), "wait");
             launch_rows(false, d_ra_, nullptr, 1, s_comp_[0]);
             mark("rowA", s_comp_[0]);
+        }
+    };
+    // Staged items of one operand lie side by side in pinned and in device memory, so the items
+    // staged since the last copy go as one copy: a copy is issued when at most one is still in
+    // flight (so the DMA engine always has the next one queued), and at the end of each operand.
+    // Fewer, larger copies pay the per-copy set-up less often; items whose operand is page-locked
+    // go one strided copy each.
+    int pend = 0;                 // first item staged but not yet copied
+    int fl_prev = -1, fl_last = -1;  // last items of the two latest copies (their ev_in_ mark completion)
+    auto in_flight = [&](int hi) {
+        if (hi < 0) return false;
+        const cudaError_t q = cudaEventQuery(ev_in_[hi]);
+        if (q == cudaErrorNotReady) {
+            if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();  // the query's answer
+            return true;
+        }
+        return false;
+    };
+    for (int i = 0; i < nin; ++i) {
+        const int P = items[i].first;
+        // the next chunk is copied by the workers while this thread issues this one
+        const bool staging = i + 1 < nin && stage_start(i + 1);
+        const bool op_end = i + 1 == nin || items[i + 1].first != P;
+        const bool flush = op_end || direct_in[P] || !merge_copies_ || !(in_flight(fl_prev) && in_flight(fl_last));
+        if (flush) {
+            const Chunk c0 = items[pend].second;
+            const size_t off = (size_t)c0.col0 * nrows * L;
+            size_t words = 0;
+            for (int k = pend; k <= i; ++k) words += (size_t)items[k].second.cw * nrows * L;
+            if (direct_in[P])
+                cuda_check(cudaMemcpy2DAsync(d_in_[P] + off, (size_t)c0.cw * L * 4, src[P] + (size_t)c0.col0 * L, pitch,
+                                             (size_t)c0.cw * L * 4, nrows, cudaMemcpyHostToDevice, s_h2d_),
+                           "H2D");
+            else
+                cuda_check(cudaMemcpyAsync(d_in_[P] + off, h_in_[P] + off, words * 4, cudaMemcpyHostToDevice, s_h2d_),
+                           "H2D");
+            cuda_check(cudaEventRecord(ev_in_[i], s_h2d_), "record");
+            mark("h2d" + std::to_string(i), s_h2d_);
+            for (int k = pend; k <= i; ++k) issue_compute(k, i);
+            fl_prev = fl_last;
+            fl_last = i;
+            pend = i + 1;
         }
         if (profile_ && i + 1 < nin) issued_us.push_back(us(clk::now()));
         if (staging) pool_->wait();

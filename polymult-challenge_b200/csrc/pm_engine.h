@@ -218,6 +218,7 @@ class Engine {
     uint32_t* h_status_ = nullptr;  // pinned copy of the device status word, written after each run_host
     bool profile_ = false;          // POLYMULT_PROFILE: per-call host and device timeline on stderr
     bool nt_gather_ = true;         // POLYMULT_GATHER_STORES=cached: ordinary stores when staging inputs
+    bool merge_copies_ = true;      // POLYMULT_MERGE_COPIES=0: one H2D copy per staged input chunk
     std::vector<cudaEvent_t> trace_ev_;  // timing events of that timeline
     cudaEvent_t ev_fused_ = nullptr;
     std::unique_ptr<HostPool> pool_;
