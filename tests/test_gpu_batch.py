@@ -105,7 +105,8 @@ def test_small_classes_against_c_oracle():
             assert np.array_equal(got[i], c_oracle_mul(k["N"], k["W"], k["q"], a[i], bb[i])), (k["N"], k["W"], i)
 
 
-@pytest.mark.parametrize("N,W", [(65536, 1747), (4096, 256), (1024, 868), (32, 64)])
+# N=16384 and 32768 at w1 = 8 run the TMA column pass with row pitches 2^6 and 2^7
+@pytest.mark.parametrize("N,W", [(65536, 1747), (32768, 100), (16384, 256), (4096, 256), (1024, 868), (32, 64)])
 def test_every_split_gives_the_same_bytes(N, W):
     torch = _torch()
     import polymult
