@@ -1022,6 +1022,7 @@ static bool host_range_pinned(const void* p, size_t bytes) {
 }
 
 void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
+    if (!pool_) throw Unsupported("this context has no host pipeline");
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
     ensure_scratch(1);
     const uint32_t nrows = plan_.nrows, ncols = plan_.ncols, L = plan_.L;
