@@ -5,6 +5,7 @@ bit-exact, on B200.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--gemm tensor|plain]
     python bench.py --profile-case [--N 65536 --W 1747 --gemm tensor --count 8 --host 0 ...]
     python bench.py --peak-int8 [--size 8192 --seconds 2]
+    python bench.py --peak-butterfly
 
 One step = one device-resident pass over a batch of BATCH multiplications whose operands
 are already in HBM (inputs 2 x BATCH x 14.4 MB > the 126 MB L2, so no flush is needed).
@@ -112,6 +113,7 @@ def parse():
     ap.add_argument("--pinned", action="store_true")
     ap.add_argument("--tune", action="store_true")
     ap.add_argument("--peak-int8", action="store_true")
+    ap.add_argument("--peak-butterfly", action="store_true")
     ap.add_argument("--size", type=int, default=8192)
     ap.add_argument("--seconds", type=float, default=2.0)
     return ap.parse_args()
@@ -820,6 +822,20 @@ def run_ours(args):
     if pipes:
         # the unit that binds the kernel, from the committed ncu capture (HBM is not it here)
         roofline["binding_pipe"] = pipes
+    if dom == "rows_fused":
+        # the row pass against the measured rate of its butterfly alone (pm_butterfly_peak): the
+        # NTT's own ceiling on this GPU, operands in registers, no memory traffic
+        try:
+            bp = polymult.butterfly_peak(local)
+            w2 = int(info["w2"])
+            bf = 3 * K * (N // 2) * w2 * B  # forward rows of a and b, inverse rows of c
+            got = bf / (stages[dom] / 1000.0)
+            roofline["butterfly"] = {"butterflies_per_launch": bf, "achieved_per_s": round(got, 0),
+                                     "peak_per_s": round(bp["bfly_per_s"], 0),
+                                     "peak_per_clk_sm": round(bp["bfly_per_clk_sm"], 2),
+                                     "frac": round(got / bp["bfly_per_s"], 4)}
+        except Exception as e:  # the peak kernel is a measurement aid, not the multiply
+            roofline["butterfly"] = {"unavailable": str(e)[:120]}
     whole = {"algorithmic_bytes_per_multiply": (12 * N * L + 24 * K * N), "ms_per_multiply": round(ms / args.steps / B, 5)}
     whole["achieved_gbs"] = round(whole["algorithmic_bytes_per_multiply"] / (whole["ms_per_multiply"] / 1000.0) / 1e9, 1)
     whole["frac_of_hbm"] = round(whole["achieved_gbs"] / peak, 4)
@@ -980,10 +996,24 @@ def run_peak_int8(a):
                       "device": torch.cuda.get_device_name(0), "corner_block_exact": ok}))
 
 
+def run_peak_butterfly(a):
+    """The NTT butterfly's rate with operands in registers over every SM (pm_butterfly_peak):
+    the ceiling of the NTT kernels, which the integer multiply-add pipe binds.  One JSON line."""
+    import torch
+    import polymult
+    r = polymult.butterfly_peak(0)
+    print(json.dumps({"butterflies_per_s": round(r["bfly_per_s"], 0), "butterflies_per_clk_sm": round(r["bfly_per_clk_sm"], 2),
+                      "method": "k_bfly_peak: bfly_ct_sh on 16 register values per thread, 2 x 512 threads per SM, "
+                                "CUDA events over 5 launches, checksum checked against the host",
+                      "device": torch.cuda.get_device_name(0)}))
+
+
 def main():
     args = parse()
     if args.profile_case:
         run_profile_case(args)
+    elif args.peak_butterfly:
+        run_peak_butterfly(args)
     elif args.peak_int8:
         run_peak_int8(args)
     elif args.impl == "reference":

@@ -297,6 +297,15 @@ int pm_test_set_status(pm_context* ctx, uint32_t bits);
  * stays usable.  Synchronous. */
 int pm_selftest_wait(int device, uint64_t limit_clocks, uint32_t* status_out);
 
+/* No reference counterpart: the measured ceiling of the NTT's arithmetic.  Runs the NTT's
+ * Harvey-Shoup butterfly (two low 32-bit multiplies, one 64-bit product, three adds) on register
+ * operands, no memory traffic, over every SM of `device`, and gives the rate in butterflies per
+ * second and per clock per SM (at the device's reported SM clock).  The NTT kernels are bound by
+ * the integer multiply-add pipe this exercises, so their butterfly rate against this one is their
+ * roofline fraction.  PM_ERR_DEVICE if the kernel's checksum differs from a host recomputation.
+ * Synchronous; a few milliseconds. */
+int pm_butterfly_peak(int device, double* bfly_per_s, double* bfly_per_clk_sm);
+
 #ifdef __cplusplus
 }
 #endif

@@ -147,6 +147,16 @@ int pm_selftest_wait(int device, uint64_t limit_clocks, uint32_t* status_out) {
     return guarded([&] { *status_out = pm::wait_selftest(device, (long long)limit_clocks); });
 }
 
+int pm_butterfly_peak(int device, double* bfly_per_s, double* bfly_per_clk_sm) {
+    if (!bfly_per_s || !bfly_per_clk_sm) return fail(PM_ERR_INVALID, "null argument");
+    DeviceScope keep;
+    return guarded([&] {
+        bool ok = false;
+        pm::butterfly_peak(device, bfly_per_s, bfly_per_clk_sm, &ok);
+        if (!ok) throw pm::DeviceCheckError("butterfly peak: the kernel's checksum differs from the host's");
+    });
+}
+
 int pm_get_info(const pm_context* ctx, pm_info* out) {
     if (!ctx || !ctx->engine || !out) return fail(PM_ERR_INVALID, "null argument");
     const pm::Engine& e = *ctx->engine;

@@ -43,6 +43,9 @@ void run_device_static(Engine& e, const uint32_t* d_a, const uint32_t* d_b, uint
 void forget_static_scratch_address(int device);
 // runs k_wait_selftest on `device` with a wait limit of `limit` clocks; returns its status word
 uint32_t wait_selftest(int device, long long limit);
+// Harvey-Shoup butterflies per second on `device` with operands in registers (k_peak.cu), per
+// clock per SM, and whether the kernel's checksum matched the host's
+void butterfly_peak(int device, double* per_s, double* per_clk_sm, bool* checked);
 
 enum GemmForm : int { GEMM_AUTO = 0, GEMM_PLAIN = 1, GEMM_TENSOR = 2, GEMM_MIXED = 3 };
 

@@ -167,6 +167,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pm_test_set_status.restype = ctypes.c_int
     lib.pm_selftest_wait.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]
     lib.pm_selftest_wait.restype = ctypes.c_int
+    lib.pm_butterfly_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.pm_butterfly_peak.restype = ctypes.c_int
     del u32p
     _lib = lib
     return lib
@@ -212,6 +214,13 @@ def wait_selftest(limit_clocks: int, device: int = 0) -> int:
     st = ctypes.c_uint32(0)
     _check(load().pm_selftest_wait(device, limit_clocks, ctypes.byref(st)))
     return st.value
+
+
+def butterfly_peak(device: int = 0) -> dict:
+    """The NTT butterfly's rate with operands in registers (pm_butterfly_peak)."""
+    a, b = ctypes.c_double(0), ctypes.c_double(0)
+    _check(load().pm_butterfly_peak(device, ctypes.byref(a), ctypes.byref(b)))
+    return {"bfly_per_s": a.value, "bfly_per_clk_sm": b.value}
 
 
 def plan_selfcheck(N: int, W: int, q_limbs) -> int:

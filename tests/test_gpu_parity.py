@@ -300,3 +300,16 @@ def test_wide_points_on_tensor_cores_in_blocks():
     assert np.array_equal(outs["auto_c"], outs["plain_c"])
     for i in range(3):
         assert np.array_equal(outs["auto_c"][i], c_oracle_mul(N, W, q, ops[i], ops[3 + i])), i
+
+
+def test_butterfly_peak_matches_the_host():
+    """pm_butterfly_peak runs the NTT's Shoup butterfly on register operands over every SM; its
+    checksum equals the host's recomputation (else PM_ERR_DEVICE), and the rate is plausible for
+    a pipe that takes the 64-bit product at a quarter of the low multiply's rate."""
+    _torch()
+    import polymult
+    ensure_library()
+    r = polymult.butterfly_peak(0)
+    assert r["bfly_per_s"] > 1e11
+    assert 2.0 < r["bfly_per_clk_sm"] < 64.0
+
