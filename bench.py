@@ -870,12 +870,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
 
-    # the legs below run on rank 0 only (no collectives; with N > 1 the other ranks are done):
-    # they describe one GPU.  The latency-measuring serving leg goes first, with torch's cached
-    # blocks released: after the batch leg (GBs of operands in torch's cache, seconds of full
-    # load) its p99 measured about twice as high.
+    # the legs below describe one GPU: they run in the one-GPU run only (with N > 1 the line
+    # carries the replicas' throughput, and the N = 1 line these legs).  The latency-measuring
+    # serving leg goes first, with torch's cached blocks released: after the batch leg (GBs of
+    # operands in torch's cache, seconds of full load) its p99 measured about twice as high.
     serving = configs = refgpu = batched = cpu = None
-    if rank == 0:
+    if rank == 0 and world == 1:
         if not args.no_serving:
             serving = run_serving(torch, args, local)
             torch.cuda.empty_cache()
