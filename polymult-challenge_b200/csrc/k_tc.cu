@@ -160,7 +160,7 @@ __device__ __forceinline__ void bulk_g2s_all(void* dst, const void* src, uint32_
 // ----------------------------------------------------------------------------------------
 // Decomposition.  Persistent, warp-specialised, 640 threads; tiles of 128 positions over
 // (batch, npos).
-//   loader group (warps 0-3): thread 0 keeps a 2-deep ring of raw coefficient tiles filled by
+//   loader group (warps 0-3): thread 0 keeps a ring of raw coefficient tiles filled by
 //     bulk copies (contiguous cnt*L words each, prefetched two tiles ahead); the group
 //     re-lays the tile out as the K-major A operand once the previous tile's MMAs have read
 //     A; thread 0 then issues the MMAs of the two prime halves -- half h once the epilogue
@@ -185,8 +185,8 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                                                               int use_bulk, int ring) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int L = P.L, kb = P.dec_kbytes, nrows_b = P.dec_nrows;
-    // ring: raw tiles in flight (2: prefetched two tiles ahead; 1: one slot, refilled once its
-    // tile is relaid, which frees shared memory for wider prime blocks)
+    // ring: raw tiles in flight (1 .. DEC_MAX_RING: each slot is refilled with the tile `ring`
+    // tiles ahead once its tile is relaid; 1 frees shared memory for wider prime blocks)
     const int KH = dec_half_primes(P.KP);                 // primes of half 0
     const int n0 = 4 * KH, n1 = nrows_b - n0;              // MMA N of the halves
     const uint32_t col1 = dec_half1_col(n0);               // TMEM column of half 1
@@ -195,8 +195,8 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
     uint32_t* raw_s = reinterpret_cast<uint32_t*>(a_s + (size_t)TC_M * kb);
     const size_t raw_words = (size_t)TC_M * L;
     uint64_t* bars = reinterpret_cast<uint64_t*>(raw_s + ring * raw_words);
-    uint64_t *bar_b = bars, *bar_raw = bars + 1, *mma_done = bars + 3, *acc_empty = bars + 5;
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bars + 7);
+    uint64_t *bar_b = bars, *bar_raw = bars + 1, *mma_done = bars + 1 + DEC_MAX_RING, *acc_empty = mma_done + 2;
+    uint32_t* slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
     volatile int* abort_f = reinterpret_cast<volatile int*>(slot + 1);
     uint2* pc_s = reinterpret_cast<uint2*>(slot + 2);  // [KP] {p, p^-1 mod 2^32}
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -214,8 +214,8 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
 
     if (threadIdx.x == 0) {
         mbar_init(bar_b, 1);
+        for (int k = 0; k < DEC_MAX_RING; ++k) mbar_init(bar_raw + k, 1);
         for (int k = 0; k < 2; ++k) {
-            mbar_init(bar_raw + k, 1);
             mbar_init(mma_done + k, 1);
             mbar_init(acc_empty + k, DEC_EPI_THREADS);
         }
@@ -258,12 +258,12 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         uint32_t i = 0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
             if (named_sync_or(1, DEC_LOAD_THREADS, *abort_f != 0)) break;
-            const int buf = ring == 2 ? (int)(i & 1) : 0;  // raw ring slot
+            const int buf = (int)(i % (uint32_t)ring);  // raw ring slot
             int cnt;
             const uint32_t* s = tile_src(tile, &cnt);
             uint32_t* raw = raw_s + buf * raw_words;
             if (use_bulk) {
-                if (wait_or_abort(bar_raw + buf, (ring == 2 ? i >> 1 : i) & 1, abort_f, P.wait_clocks) && threadIdx.x == 0)
+                if (wait_or_abort(bar_raw + buf, (i / (uint32_t)ring) & 1, abort_f, P.wait_clocks) && threadIdx.x == 0)
                     raw_pending &= ~(1u << buf);
             } else {
                 for (int w = threadIdx.x; w < cnt * L; w += DEC_LOAD_THREADS) raw[w] = __ldg(s + w);
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
                     const uint32_t* s2 = tile_src(nxt, &c2);
                     bulk_g2s_all(raw, s2, (uint32_t)c2 * L * 4, bar_raw + buf);
                     raw_pending |= 1u << buf;
-                    const uint32_t use = ring == 2 ? (i + 2) >> 1 : i + 1;  // the slot's next use
+                    const uint32_t use = (i + (uint32_t)ring) / (uint32_t)ring;  // the slot's next use
                     raw_par = (raw_par & ~(1u << buf)) | ((use & 1u) << buf);
                 }
                 bool ok = *abort_f == 0;
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(RNS_TC_THREADS, 1) k_rns_tc(DevPlan P, const u
         flag_error(P.status, DEV_ERR_WAIT);
         // copies and MMAs still in flight must land before this CTA's memory goes away
         if (!b_seen) mbar_wait_bounded(bar_b, 0, P.wait_clocks);
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < ring; ++k)
             if (raw_pending & (1u << k)) mbar_wait_bounded(bar_raw + k, (raw_par >> k) & 1u, P.wait_clocks);
         if (last_commit >= 0) mbar_wait_bounded(mma_done + last_commit, last_commit_par, P.wait_clocks);
     }
@@ -1071,7 +1071,8 @@ __global__ void __launch_bounds__(64) k_wait_selftest(uint32_t* status, long lon
 }
 
 size_t rns_tc_smem(const DevPlan& P, int ring) {
-    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + (size_t)ring * TC_M * P.L * 4 + 7 * 8 + 8 +
+    return (size_t)P.dec_nrows * P.dec_kbytes + (size_t)TC_M * P.dec_kbytes + (size_t)ring * TC_M * P.L * 4 +
+           (1 + DEC_MAX_RING + 4) * 8 + 8 +
            (size_t)P.KP * 8;
 }
 

@@ -52,6 +52,9 @@ void ntt_probe_images(int w1, int w2);              // throws CudaError if an im
 size_t ntt_cols_smem(const DevPlan& P, int ltc);
 
 // ---- plain (CUDA-core) RNS decomposition and CRT (k_rns.cu)
+// raw input tiles in flight in k_rns_tc at most (a third measured no faster at N=65536, W=1747:
+// 12.5-12.9 us per operand either way)
+constexpr int DEC_MAX_RING = 2;
 constexpr int DEC_TM = 64;   // coefficients per decomposition block (256 threads)
 constexpr int CRT_TM = 64;   // coefficients per CRT block (256 threads)
 // tab_in_smem: the block stages its constant table (digits x primes) in shared memory
