@@ -668,6 +668,9 @@ def run_batched(torch, args, local):
                 "graph_nodes": inf["graph_nodes"], "kernel_launches": inf["kernel_launches"],
                 "streams": inf["streams"], "scratch_gb": round(inf["scratch_bytes"] / 1e9, 3),
                 "gemm_forms_chosen": forms, "splits_chosen": sorted({(c["w1"], c["w2"]) for c in chosen}),
+                "variants_chosen": {"col_tma": sum(1 for c in chosen if c.get("col_tma")),
+                                    "crt_a_in_tmem": sum(1 for c in chosen if c.get("crt_tm")),
+                                    "launch_groups": sorted({int(c.get("launch_groups", 1)) for c in chosen})},
                 "class_ms": [[k["N"], k["W"], k["count"], c["gemm"], round(c["tuned_ms"], 3)]
                              for k, c in zip(ks, chosen)],
                 "matches_sequential_plain": same, "tune_cache": tune_cache or "default"})
