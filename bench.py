@@ -96,7 +96,7 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
-    ap.add_argument("--serve-requests", type=int, default=3000, help="requests per offered rate of the sweep")
+    ap.add_argument("--serve-requests", type=int, default=10000, help="requests per offered rate of the sweep")
     ap.add_argument("--serve-rates", default="2500,3500,4500", help="offered rates (requests/s) of the sweep")
     ap.add_argument("--serve-single-rate", type=float, default=600.0,
                     help="offered rate of the unbatched tensor-core comparator (one it sustains)")
@@ -862,6 +862,16 @@ def run_ours(args):
     e2e["pageable"] = e2e_leg(m, np.ascontiguousarray(host_a[0]), np.ascontiguousarray(host_b[0]),
                               np.empty((N, L), dtype=np.uint32), args.e2e_steps, world, floor_ms, want)
     e2e["pageable"]["chunk_schedule"] = pipe_pageable
+    # beside it, the reference's own schedule (solve.cu:1403-1405: eighths in with narrow heads,
+    # sixteenths out with narrow heads and tails: 10 + 10 input and 20 output chunks)
+    if not args.no_tune_pipeline:
+        m.set_pipeline(8, 16)
+        ref_sched = e2e_leg(m, np.ascontiguousarray(host_a[0]), np.ascontiguousarray(host_b[0]),
+                            np.empty((N, L), dtype=np.uint32), args.e2e_steps, world, floor_ms, want)
+        ref_sched["chunk_schedule"] = m.pipeline()
+        e2e["pageable"]["reference_schedule"] = {k: ref_sched[k] for k in ("p50_ms", "p99_ms", "p50_over_floor",
+                                                                          "matches_device_path", "chunk_schedule")}
+        m.set_pipeline(pipe_pageable["in_body"], pipe_pageable["out_body"])
     # the pageable call's second floor: its host copies (a and b gathered into page-locked
     # staging, c scattered out of it) at the host's measured copy rate with the pool's 8 threads
     hbw = host_copy_gbs(torch, 2 * N * L * 4)
